@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 bit-plane traverser (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload NAME]
+
+A step is one pass of the hot path over one batch: the headline workload
+advances a 65536 x 65536 Game of Life grid (bit planes, 512 MiB packed,
+Bernoulli(0.35) seeded input) by 1000 generations.  Under torchrun each rank
+advances its own grid of that size (independent units, no collective on the
+data path): weak scaling.
+
+value     Gcell-updates/s over all ranks, device-timed (CUDA events on the
+          launching stream), inputs resident in HBM, max over ranks.
+e2e       the same metric through the C-ABI with host buffers: every step
+          uploads the bit-plane image from pinned host memory, runs, and
+          downloads the result.
+roofline  the strip kernel against the measured integer-logic peak (the
+          binding roof for k >= 2) and against the measured HBM copy peak.
+cpu_baseline  Cellato's own CPU traverser (oracle/_ref, compiled from the
+          reference headers) on the host cores, on a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "gol-65536": dict(automaton=0, x=65536, y=65536, gens=1000, probs=[0.65, 0.35], seed=42,
+                      desc="game-of-life 65536x65536 bit_planes, Bernoulli(0.35), 1000 generations per step"),
+    "wire-32768": dict(automaton=1, x=32768, y=32768, gens=2000, probs=[0.60, 0.05, 0.05, 0.30], seed=42,
+                       desc="wire 32768x32768 bit_planes (2 planes), categorical "
+                            "(empty .60, head .05, tail .05, conductor .30), 2000 generations per step"),
+    "excitable-32768": dict(automaton=2, x=32768, y=32768, gens=2000, probs=[0.125] * 8, seed=42,
+                            desc="excitable (Greenberg-Hastings, 8 states) 32768x32768 bit_planes (3 planes), "
+                                 "uniform states, 2000 generations per step"),
+    "gol-1024": dict(automaton=0, x=1024, y=1024, gens=100, probs=[0.5, 0.5], seed=42,
+                     desc="game-of-life 1024x1024, Bernoulli(0.5), 100 generations per step"),
+}
+METRIC = "Gcell-updates/s"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "traffic.json")
+FALLBACK_HBM_GBS = 6650.0
+
+CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+# ---- clocks -----------------------------------------------------------------------------------
+
+class ClockSampler:
+    def __init__(self, gpu_index: int):
+        self.path = tempfile.mktemp(prefix="cb2_clocks_", suffix=".csv")
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={CLOCK_QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def gpu_index(local_rank: int) -> int:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [v for v in vis.split(",") if v.strip()]
+        if local_rank < len(ids) and ids[local_rank].strip().isdigit():
+            return int(ids[local_rank])
+    return local_rank
+
+
+# ---- CPU baseline: Cellato's own CPU traverser ------------------------------------------------
+
+def cpu_sample(automaton: int, probs, target_s: float, threads: int | None = None) -> dict:
+    """Times the reference CPU simple traverser (bit_planes, 64-bit words) with
+    one independent grid per host thread on a 4096x4096 sample."""
+    from oracle import oracle as O
+
+    threads = threads or os.cpu_count() or 1
+    x = y = 4096
+    cells = O.init_cells(x, y, 1, O.thresholds(probs))
+    if O.ref_available():
+        kind = "reference"
+        run = lambda gens: O.ref_bench(automaton, cells, gens, threads, "bit_planes", 64)  # noqa: E731
+    else:  # the C restatement, single-threaded
+        kind, threads = "port", 1
+        planes = O.pack("bit_planes", cells, O.PLANES[automaton], 32).view("uint32")
+
+        def run(gens):
+            t0 = time.perf_counter()
+            O.run_bit_planes(automaton, planes, x, y, gens)
+            return time.perf_counter() - t0
+    probe = max(run(2), 1e-4)
+    gens = max(2, int(target_s / probe * 2))
+    secs = run(gens)
+    value = threads * x * y * gens / secs / 1e9
+    return {"value": value, "unit": METRIC, "cores": threads, "kind": kind,
+            "sample": f"{threads} host thread(s), each its own {x}x{y} grid, {gens} generations, "
+                      f"Cellato CPU simple traverser, bit_planes layout, 64-bit words ({secs:.2f} s)"}
+
+
+def reference_arm(args, wl) -> None:
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    target = 8.0
+    samples = []
+    for _ in range(args.warmup):
+        cpu_sample(wl["automaton"], wl["probs"], 1.0)
+    for _ in range(args.steps):
+        samples.append(cpu_sample(wl["automaton"], wl["probs"], target))
+    value = statistics.mean(s["value"] for s in samples)
+    base = dict(samples[-1])
+    base["value"] = value
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+           "config": {"workload": wl["desc"], "sample": base["sample"]},
+           "cpu_baseline": base, "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
+                                         "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+# ---- the B200 arm ------------------------------------------------------------------------------
+
+def measured_peaks() -> dict:
+    try:
+        with open(PEAKS_FILE) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def traffic_for(kernel_key: str):
+    try:
+        with open(TRAFFIC_FILE) as f:
+            t = json.load(f)
+        return t.get(kernel_key)
+    except (OSError, ValueError):
+        return None
+
+
+def launches_per_run(gens: int, k: int) -> int:
+    n, left = 0, gens
+    while left > 0:
+        step = k if left >= k else (4 if left >= 4 else 2 if left >= 2 else 1)
+        left -= step
+        n += 1
+    return n
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="gol-65536", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return reference_arm(args, wl)
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be at least 3")
+
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local_rank = dist_env()
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+
+    import cellato_b200 as cb
+
+    a, x, y, gens = wl["automaton"], wl["x"], wl["y"], wl["gens"]
+    name, P, _ = cb.automaton_info(a)
+    cells = x * y
+    stream = torch.cuda.current_stream()
+    tuned = cb.autotune(a, x, y, budget_ms=4000)
+    plan = cb.plan(a, x, y)
+    k = plan["temporal_steps"]
+    grid = cb.DeviceGrid(a, x, y)
+    grid.fill_random(wl["seed"] + rank, wl["probs"], stream=stream)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident timing ----
+    for _ in range(args.warmup):
+        grid.run(gens, stream=stream)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(gpu_index(local_rank)) if local_rank == 0 else None
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        grid.run(gens, stream=stream)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop() if sampler else None
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    value = world * cells * gens * args.steps / (ms * 1e-3) / 1e9
+    launches = launches_per_run(gens, k) * args.steps
+
+    # ---- roofline of the strip kernel ----
+    avg_launch_s = ms * 1e-3 / launches
+    gens_per_launch = gens * args.steps / launches
+    bytes_per_launch = 2 * P * cells / 8  # read + write every plane once
+    hbm_gbs = bytes_per_launch / avg_launch_s / 1e9
+    peaks = measured_peaks()
+    hbm_peak = peaks.get("hbm_gbs", FALLBACK_HBM_GBS)
+    lop3_peak = cb.measure_lop3_peak()
+    alu_per_word, shfl_per_word = cb.network_ops(a)
+    int_ops_per_launch = alu_per_word * (cells / 32) * gens_per_launch
+    int_gops = int_ops_per_launch / avg_launch_s / 1e9
+    int_frac = int_gops / (lop3_peak / 1e9)
+    hbm_frac = hbm_gbs / hbm_peak
+    kernel_key = f"strip_kernel<{name},K={k},V={plan['words_per_lane']}>@{x}x{y}"
+    traffic = traffic_for(kernel_key)
+    roof = {
+        "bound": "int" if int_frac >= hbm_frac else "hbm",
+        "kernel": kernel_key,
+        "achieved": int_gops if int_frac >= hbm_frac else hbm_gbs,
+        "peak": lop3_peak / 1e9 if int_frac >= hbm_frac else hbm_peak,
+        "unit": "Gop/s" if int_frac >= hbm_frac else "GB/s",
+        "frac": max(int_frac, hbm_frac),
+        "traffic": traffic,
+        "peak_source": ("measured LOP3 issue rate (cb2_measure_lop3_peak, this run)" if int_frac >= hbm_frac else
+                        ("measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback 6.65 TB/s")),
+        "int": {"achieved_gops": int_gops, "peak_gops": lop3_peak / 1e9, "frac": int_frac,
+                "ops_per_word_per_generation": alu_per_word, "shuffles_per_word_per_generation": shfl_per_word},
+        "hbm": {"achieved_gbs": hbm_gbs, "peak_gbs": hbm_peak, "frac": hbm_frac,
+                "algorithmic_bytes_per_launch": bytes_per_launch,
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
+        "avg_launch_ms": avg_launch_s * 1e3,
+        "generations_per_launch": gens_per_launch,
+    }
+
+    # ---- end to end through the C-ABI with host buffers ----
+    nbytes = cb.layout_bytes(a, "bit_planes", 64, x, y)
+    host_in = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    host_out = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    grid.download("bit_planes", 64, stream=stream, out=host_in.numpy())
+    host_img = cb.HostGrid(a, "bit_planes", 64, x, y, host_in.numpy())
+    for _ in range(1):
+        grid.upload(host_img, stream=stream)
+        grid.run(gens, stream=stream)
+        grid.download("bit_planes", 64, stream=stream, out=host_out.numpy())
+    torch.cuda.synchronize()
+    barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.perf_counter()
+    f0.record(stream)
+    for _ in range(args.steps):
+        grid.upload(host_img, stream=stream)
+        grid.run(gens, stream=stream)
+        grid.download("bit_planes", 64, stream=stream, out=host_out.numpy())
+    f1.record(stream)
+    f1.synchronize()
+    wall = time.perf_counter() - w0
+    barrier()
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1))
+    e2e_wall = max_over_ranks(wall)
+    e2e_value = world * cells * gens * args.steps / (e2e_ms * 1e-3) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_sample(a, wl["probs"], args.cpu_seconds)
+
+    grid.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    out = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": wl["desc"], "automaton": name, "x_size": x, "y_size": y,
+                   "generations_per_step": gens, "plan": plan, "autotuned": tuned,
+                   "l2": "inputs larger than L2 (each plane buffer is 512 MiB at 65536^2)",
+                   "parallelism": f"replicas x{world} (one grid per GPU)" if world > 1 else "single GPU"},
+        "roofline": roof,
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                "wall_s": e2e_wall, "path": "cb2_grid_upload(bit_planes) + cb2_grid_run + cb2_grid_download, "
+                                            "pinned host buffers"},
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,142 @@
+"""ctypes binding of the C-ABI in ``include/cellato_b200.h``.
+
+The library ``libcellato_b200.so`` is built in-tree (``__graft_entry__.build()``
+or ``make -C cellato_b200/csrc``).  There is no fallback: if the library is
+missing, importing this module raises ``ImportError``.
+
+Status codes become the exception types the reference raises for the same
+conditions: ``CudaError`` for CUDA failures (traversers/cuda_utils.cuh:37-47),
+``ValueError`` for invalid arguments (std::invalid_argument), ``LookupError``
+for unknown names, ``MemoryError`` for exhausted device memory and
+``TimeoutError`` for bounded device waits that gave up.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcellato_b200.so")
+HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "cellato_b200.h")
+
+CB2_OK = 0
+CB2_EINVAL = -1
+CB2_ECUDA = -2
+CB2_ENOMEM = -3
+CB2_ESTATE = -4
+CB2_ETIMEOUT = -5
+CB2_ENOTFOUND = -6
+
+LAYOUT_STANDARD = 0
+LAYOUT_BIT_ARRAY = 1
+LAYOUT_BIT_PLANES = 2
+LAYOUT_TILED_BIT_PLANES = 3
+LAYOUTS = {
+    "standard": LAYOUT_STANDARD,
+    "bit_array": LAYOUT_BIT_ARRAY,
+    "bit_planes": LAYOUT_BIT_PLANES,
+    "tiled_bit_planes": LAYOUT_TILED_BIT_PLANES,
+}
+
+
+class CudaError(RuntimeError):
+    """A CUDA runtime call inside the library failed."""
+
+
+class StateError(ValueError):
+    """A cell value is not an index of the automaton's state dictionary."""
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("temporal_steps", ctypes.c_int), ("tile_rows", ctypes.c_int), ("words_per_lane", ctypes.c_int)]
+
+    def as_dict(self):
+        return {"temporal_steps": self.temporal_steps, "tile_rows": self.tile_rows,
+                "words_per_lane": self.words_per_lane}
+
+
+_i64 = ctypes.c_int64
+_vp = ctypes.c_void_p
+_vpp = ctypes.POINTER(ctypes.c_void_p)
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_tp = ctypes.POINTER(Tuning)
+
+# name -> (restype, argtypes)
+_SIGNATURES = {
+    "cb2_abi_version": (ctypes.c_int, []),
+    "cb2_last_error": (ctypes.c_char_p, []),
+    "cb2_automaton_lookup": (ctypes.c_int, [ctypes.c_char_p]),
+    "cb2_automaton_info": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
+                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "cb2_run_bit_planes": (ctypes.c_int, [ctypes.c_int, _vpp, _vpp, _i64, _i64, _i64, _tp, _vp,
+                                          ctypes.POINTER(ctypes.c_int)]),
+    "cb2_grid_create": (ctypes.c_int, [ctypes.c_int, _i64, _i64, ctypes.POINTER(_vp)]),
+    "cb2_grid_destroy": (ctypes.c_int, [_vp]),
+    "cb2_grid_upload": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_size_t, _vp]),
+    "cb2_grid_download": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_size_t, _vp]),
+    "cb2_layout_bytes": (_i64, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _i64, _i64]),
+    "cb2_grid_fill_random": (ctypes.c_int, [_vp, ctypes.c_uint64, _u64p, ctypes.c_int, _vp]),
+    "cb2_grid_run": (ctypes.c_int, [_vp, _i64, _tp, _vp]),
+    "cb2_grid_checksum": (ctypes.c_int, [_vp, _i64p, ctypes.c_int, _u64p, _vp]),
+    "cb2_grid_planes": (ctypes.c_int, [_vp, _vpp, ctypes.POINTER(ctypes.c_int), _i64p]),
+    "cb2_grid_time_step": (_i64, [_vp]),
+    "cb2_autotune": (ctypes.c_int, [ctypes.c_int, _i64, _i64, ctypes.c_double, _tp]),
+    "cb2_tuning_load": (ctypes.c_int, [ctypes.c_char_p]),
+    "cb2_tuning_save": (ctypes.c_int, [ctypes.c_char_p]),
+    "cb2_plan": (ctypes.c_int, [ctypes.c_int, _i64, _i64, _tp, _tp]),
+    "cb2_measure_lop3_peak": (ctypes.c_int, [ctypes.POINTER(ctypes.c_double)]),
+    "cb2_network_ops": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                       ctypes.POINTER(ctypes.c_double)]),
+}
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is not built; run `python -c 'import __graft_entry__ as g; g.build()'` "
+                          "or `make -C cellato_b200/csrc` (there is no CPU fallback)")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def last_error() -> str:
+    msg = lib.cb2_last_error()
+    return msg.decode() if msg else ""
+
+
+def check(rc: int, what: str = "") -> int:
+    """Raise the exception matching a negative status code; return rc otherwise."""
+    if rc >= 0:
+        return rc
+    msg = last_error()
+    text = f"{what}: {msg}" if what else msg
+    if rc == CB2_ECUDA:
+        raise CudaError(text)
+    if rc == CB2_ESTATE:
+        raise StateError(text)
+    if rc == CB2_ENOMEM:
+        raise MemoryError(text)
+    if rc == CB2_ETIMEOUT:
+        raise TimeoutError(text)
+    if rc == CB2_ENOTFOUND:
+        raise LookupError(text)
+    raise ValueError(text)
+
+
+def declared_symbols() -> list[str]:
+    """Function names the public header declares (for the ABI export test)."""
+    with open(HEADER_PATH) as f:
+        text = f.read()
+    return sorted(set(re.findall(r"\b(cb2_[a-z0-9_]+)\s*\(", text)))
+
+
+def tuning(temporal_steps: int = 0, tile_rows: int = 0, words_per_lane: int = 0) -> Tuning:
+    return Tuning(temporal_steps, tile_rows, words_per_lane)

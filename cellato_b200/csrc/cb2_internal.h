@@ -1,0 +1,74 @@
+// cb2_internal.h -- declarations shared by the library's translation units.
+// Not part of the public C-ABI (include/cellato_b200.h is).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+namespace cb2 {
+
+constexpr int kMaxPlanes = 3;
+constexpr int kNumAutomata = 3;
+constexpr int kMaxThresholds = 7;  // up to 8 states
+constexpr int kStripWarpsPerBlock = 4;
+
+// Geometry of one device grid: P planes of h rows x wd 32-bit words.
+struct grid_geom {
+    int automaton;
+    int planes;
+    int64_t x_size, y_size;  // cells
+    int32_t wd, h;           // 32-bit words per row, rows
+    int64_t plane_words;     // wd * h
+};
+
+// Tuning knobs for one single-grid run.
+struct run_plan {
+    int k;          // generations per launch (1, 2, 4 or 8)
+    int v;          // words per lane (1 or 2)
+    int tile_rows;  // output rows per strip task
+};
+
+int planes_of(int automaton);
+const char* name_of(int automaton);
+int find_automaton(const char* name);
+
+// Launches one K-generation strip pass over a whole grid (in -> out).
+cudaError_t launch_strip_pass(const grid_geom& g, const uint32_t* in, uint32_t* out, const run_plan& plan,
+                              cudaStream_t stream);
+// Strip tasks per column and per row for a plan, and the number of tasks.
+void strip_counts(const grid_geom& g, int v, int tile_rows, int* nsx, int* nsy);
+// Output rows per task so that one launch fills the GPU about once.
+int auto_tile_rows(const grid_geom& g, int k, int v);
+// Registers-limited number of resident strip warps on this device.
+int resident_strip_warps(int automaton, int k, int v);
+
+// Layout conversions between host images and device planes (device -> device).
+cudaError_t launch_pack_cells(const grid_geom& g, const void* cells, int cell_bytes, uint32_t* planes,
+                              unsigned* bad_flag, cudaStream_t s);
+cudaError_t launch_unpack_cells(const grid_geom& g, const uint32_t* planes, void* cells, int cell_bytes,
+                                cudaStream_t s);
+cudaError_t launch_bit_array_to_planes(const grid_geom& g, const void* words, int word_bits, uint32_t* planes,
+                                       cudaStream_t s);
+cudaError_t launch_planes_to_bit_array(const grid_geom& g, const uint32_t* planes, void* words, int word_bits,
+                                       cudaStream_t s);
+cudaError_t launch_tiled_to_planes(const grid_geom& g, const void* tiled, int word_bits, uint32_t* planes,
+                                   cudaStream_t s);
+cudaError_t launch_planes_to_tiled(const grid_geom& g, const uint32_t* planes, void* tiled, int word_bits,
+                                   cudaStream_t s);
+cudaError_t launch_fill_random(const grid_geom& g, uint32_t* planes, uint64_t seed, const uint64_t* thr, int nthr,
+                               cudaStream_t s);
+// Adds the 16 tile sums of state values into sums[16] (which the caller zeroes).
+cudaError_t launch_checksum(const grid_geom& g, const uint32_t* planes, const int64_t* values, int nvalues,
+                            unsigned long long* sums, cudaStream_t s);
+
+// Integer-pipe peak probe: `iters` rounds of independent 3-input logic ops.
+cudaError_t launch_lop3_probe(uint32_t* sink, int blocks, int threads, int iters, cudaStream_t s);
+// Logic ops one lane of the probe kernel issues per iteration.
+constexpr int kLop3ProbeOpsPerIter = 64;
+
+// Thread-local error message for cb2_last_error().
+void set_error(const std::string& msg);
+
+} // namespace cb2

@@ -1,0 +1,499 @@
+// cb2_kernels.cu -- device kernels of the library and their launchers.
+//
+//  * strip_kernel<Rule, K, V>   the hot path (cb2_strip.cuh), K generations
+//                               per launch over a whole grid
+//  * layout conversion kernels  standard / bit_array / tiled host images to
+//                               and from the device's linear bit planes
+//  * fill_random_kernel         the seeded SplitMix64 input generator
+//  * checksum_kernel            the reference's 16-tile checksum from planes
+//  * lop3_probe_kernel          integer-pipe peak probe for the roofline
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <mutex>
+
+#include "cb2_internal.h"
+#include "cb2_rules.cuh"
+#include "cb2_strip.cuh"
+
+namespace cb2 {
+
+// ---------------------------------------------------------------------------
+// Strip pass
+// ---------------------------------------------------------------------------
+
+struct strip_launch {
+    const uint32_t* in;
+    uint32_t* out;
+    int64_t plane_words;
+    int32_t wd, h;
+    int32_t nsx, nsy, tile_rows;
+};
+
+template <class R, int K, int V>
+__global__ void __launch_bounds__(kStripWarpsPerBlock * 32) strip_kernel(strip_launch a) {
+    const int warp = blockIdx.x * kStripWarpsPerBlock + (threadIdx.x >> 5);
+    if (warp >= a.nsx * a.nsy) return;  // whole warps only
+    constexpr int own = 32 * V - 2;
+    const int sx = warp % a.nsx, sy = warp / a.nsx;
+    strip_task t;
+    t.in = a.in;
+    t.out = a.out;
+    t.plane_words = a.plane_words;
+    t.wd = a.wd;
+    t.h = a.h;
+    t.x0 = sx * own;
+    t.nx = min(own, a.wd - t.x0);
+    t.y0 = sy * a.tile_rows;
+    t.ny = min(a.tile_rows, a.h - t.y0);
+    strip_run<R, K, V>(t);
+}
+
+using strip_fn = void (*)(strip_launch);
+
+template <class R>
+static strip_fn strip_for(int klog, int v) {
+    static const strip_fn table[4][2] = {
+        {strip_kernel<R, 1, 1>, strip_kernel<R, 1, 2>},
+        {strip_kernel<R, 2, 1>, strip_kernel<R, 2, 2>},
+        {strip_kernel<R, 4, 1>, strip_kernel<R, 4, 2>},
+        {strip_kernel<R, 8, 1>, strip_kernel<R, 8, 2>},
+    };
+    return table[klog][v - 1];
+}
+
+static int klog_of(int k) { return k == 1 ? 0 : k == 2 ? 1 : k == 4 ? 2 : k == 8 ? 3 : -1; }
+
+static strip_fn strip_kernel_for(int automaton, int k, int v) {
+    const int kl = klog_of(k);
+    if (kl < 0 || v < 1 || v > 2) return nullptr;
+    switch (automaton) {
+    case 0: return strip_for<game_of_life>(kl, v);
+    case 1: return strip_for<wire>(kl, v);
+    case 2: return strip_for<excitable>(kl, v);
+    default: return nullptr;
+    }
+}
+
+int planes_of(int automaton) {
+    switch (automaton) {
+    case 0: return game_of_life::P;
+    case 1: return wire::P;
+    case 2: return excitable::P;
+    default: return -1;
+    }
+}
+
+void strip_counts(const grid_geom& g, int v, int tile_rows, int* nsx, int* nsy) {
+    const int own = 32 * v - 2;
+    *nsx = (g.wd + own - 1) / own;
+    *nsy = (g.h + tile_rows - 1) / tile_rows;
+}
+
+int resident_strip_warps(int automaton, int k, int v) {
+    static std::mutex mu;
+    static int cache[kNumAutomata][4][2] = {};
+    static int sms = 0;
+    const int kl = klog_of(k);
+    if (kl < 0 || automaton < 0 || automaton >= kNumAutomata || v < 1 || v > 2) return 0;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 1;
+    }
+    int& slot = cache[automaton][kl][v - 1];
+    if (!slot) {
+        int blocks = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, strip_kernel_for(automaton, k, v),
+                                                      kStripWarpsPerBlock * 32, 0);
+        slot = std::max(1, blocks) * kStripWarpsPerBlock * sms;
+    }
+    return slot;
+}
+
+int auto_tile_rows(const grid_geom& g, int k, int v) {
+    const int resident = resident_strip_warps(g.automaton, k, v);
+    int nsx, nsy;
+    strip_counts(g, v, 1, &nsx, &nsy);
+    // One wave: as many row tasks per column as fit beside the other columns.
+    const int per_column = std::max(1, resident / std::max(1, nsx));
+    int rows = (g.h + per_column - 1) / per_column;
+    // Keep the 2K halo rows of each task small against its own rows.
+    rows = std::max(rows, 8 * k);
+    return std::min(rows, (int)g.h);
+}
+
+cudaError_t launch_strip_pass(const grid_geom& g, const uint32_t* in, uint32_t* out, const run_plan& plan,
+                              cudaStream_t stream) {
+    strip_fn fn = strip_kernel_for(g.automaton, plan.k, plan.v);
+    if (!fn) return cudaErrorInvalidValue;
+    strip_launch a;
+    a.in = in;
+    a.out = out;
+    a.plane_words = g.plane_words;
+    a.wd = g.wd;
+    a.h = g.h;
+    a.tile_rows = plan.tile_rows;
+    strip_counts(g, plan.v, plan.tile_rows, &a.nsx, &a.nsy);
+    const int64_t tasks = (int64_t)a.nsx * a.nsy;
+    const unsigned blocks = (unsigned)((tasks + kStripWarpsPerBlock - 1) / kStripWarpsPerBlock);
+    fn<<<blocks, kStripWarpsPerBlock * 32, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Seeded input generator: cell i = y*X + x draws u = mix(seed + (i+1)*gamma)
+// >> 11 (SplitMix64, 53 uniform bits); its state index is the number of
+// cumulative thresholds <= u.
+// ---------------------------------------------------------------------------
+
+struct thr_pack {
+    unsigned long long t[kMaxThresholds];
+    int n;
+};
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+__global__ void fill_random_kernel(uint32_t* planes, int64_t plane_words, int32_t wd, int64_t x_size, int P,
+                                   uint64_t seed, thr_pack thr) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < plane_words; w += stride) {
+        const int64_t y = w / wd, xw = w - y * wd;
+        const uint64_t i0 = (uint64_t)(y * x_size + xw * 32);
+        uint32_t out[kMaxPlanes] = {0, 0, 0};
+#pragma unroll 4
+        for (int j = 0; j < 32; ++j) {
+            const uint64_t u = mix64(seed + (i0 + j + 1) * 0x9E3779B97F4A7C15ull) >> 11;
+            uint32_t s = 0;
+            for (int t = 0; t < thr.n; ++t) s += u >= thr.t[t];
+#pragma unroll
+            for (int p = 0; p < kMaxPlanes; ++p) out[p] |= ((s >> p) & 1u) << j;
+        }
+        for (int p = 0; p < P; ++p) planes[p * plane_words + w] = out[p];
+    }
+}
+
+static unsigned grid_for(int64_t items, int threads) {
+    const int64_t b = (items + threads - 1) / threads;
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 64));
+}
+
+cudaError_t launch_fill_random(const grid_geom& g, uint32_t* planes, uint64_t seed, const uint64_t* thr, int nthr,
+                               cudaStream_t s) {
+    if (nthr < 0 || nthr > kMaxThresholds) return cudaErrorInvalidValue;
+    thr_pack tp{};
+    for (int i = 0; i < nthr; ++i) tp.t[i] = thr[i];
+    tp.n = nthr;
+    fill_random_kernel<<<grid_for(g.plane_words, 256), 256, 0, s>>>(planes, g.plane_words, g.wd, g.x_size, g.planes,
+                                                                     seed, tp);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Standard layout (one state index per cell, 1 or 4 bytes) <-> planes.
+// Thread per 32-cell plane word; rows are whole words (x_size % 32 == 0).
+// ---------------------------------------------------------------------------
+
+template <typename cell_t>
+__global__ void pack_cells_kernel(const cell_t* __restrict__ cells, int64_t plane_words, int32_t wd, int64_t x_size,
+                                  int P, uint32_t* __restrict__ planes, unsigned* bad) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const uint32_t max_state = (1u << P) - 1u;
+    for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < plane_words; w += stride) {
+        const int64_t y = w / wd, xw = w - y * wd;
+        const cell_t* src = cells + y * x_size + xw * 32;
+        uint32_t out[kMaxPlanes] = {0, 0, 0};
+        bool any_bad = false;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            const uint32_t s = (uint32_t)src[j];
+            any_bad |= s > max_state;
+#pragma unroll
+            for (int p = 0; p < kMaxPlanes; ++p) out[p] |= ((s >> p) & 1u) << j;
+        }
+        if (any_bad) atomicOr(bad, 1u);
+        for (int p = 0; p < P; ++p) planes[p * plane_words + w] = out[p];
+    }
+}
+
+template <typename cell_t>
+__global__ void unpack_cells_kernel(const uint32_t* __restrict__ planes, int64_t plane_words, int32_t wd,
+                                    int64_t x_size, int P, cell_t* __restrict__ cells) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < plane_words; w += stride) {
+        const int64_t y = w / wd, xw = w - y * wd;
+        uint32_t in[kMaxPlanes] = {0, 0, 0};
+        for (int p = 0; p < P; ++p) in[p] = planes[p * plane_words + w];
+        cell_t* dst = cells + y * x_size + xw * 32;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            uint32_t s = 0;
+#pragma unroll
+            for (int p = 0; p < kMaxPlanes; ++p) s |= ((in[p] >> j) & 1u) << p;
+            dst[j] = (cell_t)s;
+        }
+    }
+}
+
+cudaError_t launch_pack_cells(const grid_geom& g, const void* cells, int cell_bytes, uint32_t* planes,
+                              unsigned* bad_flag, cudaStream_t s) {
+    const unsigned blocks = grid_for(g.plane_words, 256);
+    if (cell_bytes == 1)
+        pack_cells_kernel<uint8_t><<<blocks, 256, 0, s>>>((const uint8_t*)cells, g.plane_words, g.wd, g.x_size,
+                                                           g.planes, planes, bad_flag);
+    else if (cell_bytes == 4)
+        pack_cells_kernel<uint32_t><<<blocks, 256, 0, s>>>((const uint32_t*)cells, g.plane_words, g.wd, g.x_size,
+                                                            g.planes, planes, bad_flag);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack_cells(const grid_geom& g, const uint32_t* planes, void* cells, int cell_bytes,
+                                cudaStream_t s) {
+    const unsigned blocks = grid_for(g.plane_words, 256);
+    if (cell_bytes == 1)
+        unpack_cells_kernel<uint8_t><<<blocks, 256, 0, s>>>(planes, g.plane_words, g.wd, g.x_size, g.planes,
+                                                             (uint8_t*)cells);
+    else if (cell_bytes == 4)
+        unpack_cells_kernel<uint32_t><<<blocks, 256, 0, s>>>(planes, g.plane_words, g.wd, g.x_size, g.planes,
+                                                              (uint32_t*)cells);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// bit_array layout (memory/bit_array_grid.hpp:80-333): cells_per_word =
+// W / P whole states per W-bit word, cell i = y*X + x at word i / cpw, bit
+// (i % cpw) * P.  A word never spans two rows (X % cpw == 0).
+// ---------------------------------------------------------------------------
+
+template <typename word_t>
+__global__ void bit_array_to_planes_kernel(const word_t* __restrict__ words, int64_t plane_words, int32_t wd,
+                                           int64_t x_size, int P, uint32_t* __restrict__ planes) {
+    constexpr int W = sizeof(word_t) * 8;
+    const int cpw = W / P;
+    const word_t mask = (word_t)((1u << P) - 1u);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < plane_words; w += stride) {
+        const int64_t y = w / wd, xw = w - y * wd;
+        const int64_t i0 = y * x_size + xw * 32;
+        int64_t wi = i0 / cpw;
+        int r = (int)(i0 - wi * cpw);
+        word_t cur = words[wi];
+        uint32_t out[kMaxPlanes] = {0, 0, 0};
+        for (int j = 0; j < 32; ++j) {
+            const uint32_t s = (uint32_t)((cur >> (r * P)) & mask);
+#pragma unroll
+            for (int p = 0; p < kMaxPlanes; ++p) out[p] |= ((s >> p) & 1u) << j;
+            if (++r == cpw && j < 31) {
+                r = 0;
+                cur = words[++wi];
+            }
+        }
+        for (int p = 0; p < P; ++p) planes[p * plane_words + w] = out[p];
+    }
+}
+
+template <typename word_t>
+__global__ void planes_to_bit_array_kernel(const uint32_t* __restrict__ planes, int64_t plane_words, int32_t wd,
+                                           int64_t x_size, int64_t n_words, int P, word_t* __restrict__ words) {
+    constexpr int W = sizeof(word_t) * 8;
+    const int cpw = W / P;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t wi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; wi < n_words; wi += stride) {
+        const int64_t i0 = wi * cpw;
+        const int64_t y = i0 / x_size, x0 = i0 - y * x_size;
+        word_t out = 0;
+        int64_t pw = -1;
+        uint32_t in[kMaxPlanes] = {0, 0, 0};
+        for (int j = 0; j < cpw; ++j) {
+            const int64_t x = x0 + j;
+            if ((x >> 5) != pw) {
+                pw = x >> 5;
+                for (int p = 0; p < P; ++p) in[p] = planes[p * plane_words + y * wd + pw];
+            }
+            word_t s = 0;
+            for (int p = 0; p < P; ++p) s |= (word_t)((in[p] >> (x & 31)) & 1u) << p;
+            out |= s << (j * P);
+        }
+        words[wi] = out;
+    }
+}
+
+cudaError_t launch_bit_array_to_planes(const grid_geom& g, const void* words, int word_bits, uint32_t* planes,
+                                       cudaStream_t s) {
+    const unsigned blocks = grid_for(g.plane_words, 256);
+    if (word_bits == 32)
+        bit_array_to_planes_kernel<uint32_t><<<blocks, 256, 0, s>>>((const uint32_t*)words, g.plane_words, g.wd,
+                                                                     g.x_size, g.planes, planes);
+    else if (word_bits == 64)
+        bit_array_to_planes_kernel<unsigned long long><<<blocks, 256, 0, s>>>(
+            (const unsigned long long*)words, g.plane_words, g.wd, g.x_size, g.planes, planes);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_planes_to_bit_array(const grid_geom& g, const uint32_t* planes, void* words, int word_bits,
+                                       cudaStream_t s) {
+    const int cpw = word_bits / g.planes;
+    const int64_t n_words = g.x_size * g.y_size / cpw;
+    const unsigned blocks = grid_for(n_words, 256);
+    if (word_bits == 32)
+        planes_to_bit_array_kernel<uint32_t><<<blocks, 256, 0, s>>>(planes, g.plane_words, g.wd, g.x_size, n_words,
+                                                                     g.planes, (uint32_t*)words);
+    else if (word_bits == 64)
+        planes_to_bit_array_kernel<unsigned long long><<<blocks, 256, 0, s>>>(
+            planes, g.plane_words, g.wd, g.x_size, n_words, g.planes, (unsigned long long*)words);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// tiled_bit_planes layout (memory/tiled_bit_planes_grid.hpp:244-287): a W-bit
+// word is an 8 x (W/8) tile, bit (x%8) + 8*(y%th).  Byte r of tile word
+// (xt, yt) is therefore byte xt of linear row yt*th + r: a byte gather.
+// ---------------------------------------------------------------------------
+
+__global__ void tiled_to_planes_kernel(const uint8_t* __restrict__ tiled, int64_t plane_words, int32_t wd,
+                                       int64_t x_size, int th, int P, uint32_t* __restrict__ planes) {
+    const int64_t xt_n = x_size / 8;
+    const int64_t plane_bytes = plane_words * 4;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < plane_words; w += stride) {
+        const int64_t y = w / wd, xw = w - y * wd;
+        const int64_t base = ((y / th) * xt_n + xw * 4) * th + (y % th);
+        for (int p = 0; p < P; ++p) {
+            const uint8_t* src = tiled + p * plane_bytes + base;
+            planes[p * plane_words + w] = (uint32_t)src[0] | ((uint32_t)src[th] << 8) |
+                                          ((uint32_t)src[2 * th] << 16) | ((uint32_t)src[3 * th] << 24);
+        }
+    }
+}
+
+__global__ void planes_to_tiled_kernel(const uint32_t* __restrict__ planes, int64_t plane_words, int32_t wd,
+                                       int64_t x_size, int th, int P, uint8_t* __restrict__ tiled) {
+    const int64_t xt_n = x_size / 8;
+    const int64_t plane_bytes = plane_words * 4;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < plane_words; w += stride) {
+        const int64_t y = w / wd, xw = w - y * wd;
+        const int64_t base = ((y / th) * xt_n + xw * 4) * th + (y % th);
+        for (int p = 0; p < P; ++p) {
+            const uint32_t v = planes[p * plane_words + w];
+            uint8_t* dst = tiled + p * plane_bytes + base;
+            dst[0] = (uint8_t)v;
+            dst[th] = (uint8_t)(v >> 8);
+            dst[2 * th] = (uint8_t)(v >> 16);
+            dst[3 * th] = (uint8_t)(v >> 24);
+        }
+    }
+}
+
+cudaError_t launch_tiled_to_planes(const grid_geom& g, const void* tiled, int word_bits, uint32_t* planes,
+                                   cudaStream_t s) {
+    if (word_bits != 32 && word_bits != 64) return cudaErrorInvalidValue;
+    tiled_to_planes_kernel<<<grid_for(g.plane_words, 256), 256, 0, s>>>(
+        (const uint8_t*)tiled, g.plane_words, g.wd, g.x_size, word_bits / 8, g.planes, planes);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_planes_to_tiled(const grid_geom& g, const uint32_t* planes, void* tiled, int word_bits,
+                                   cudaStream_t s) {
+    if (word_bits != 32 && word_bits != 64) return cudaErrorInvalidValue;
+    planes_to_tiled_kernel<<<grid_for(g.plane_words, 256), 256, 0, s>>>(planes, g.plane_words, g.wd, g.x_size,
+                                                                        word_bits / 8, g.planes, (uint8_t*)tiled);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Checksum (memory/standard_grid.hpp:182-218): 4 x 4 tiles of ceil(X/4) x
+// ceil(Y/4) cells, sum of state VALUES per tile.  Counted from the planes
+// with popcounts of per-state minterms under per-tile column masks.
+// ---------------------------------------------------------------------------
+
+struct value_pack {
+    long long v[1 << kMaxPlanes];
+};
+
+__global__ void checksum_kernel(const uint32_t* __restrict__ planes, int64_t plane_words, int32_t wd,
+                                int64_t x_size, int64_t y_size, int P, value_pack vals,
+                                unsigned long long* sums) {
+    __shared__ unsigned long long acc[16];
+    if (threadIdx.x < 16) acc[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t tw = (x_size + 3) / 4, th = (y_size + 3) / 4;
+    const int nstates = 1 << P;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < plane_words; w += stride) {
+        const int64_t y = w / wd, xw = w - y * wd;
+        const int ty = (int)(y / th);
+        uint32_t in[kMaxPlanes] = {0, 0, 0};
+        for (int p = 0; p < P; ++p) in[p] = planes[p * plane_words + w];
+        const int64_t x0 = xw * 32, x1 = x0 + 32;
+        for (int64_t tx = x0 / tw; tx < 4 && tx * tw < x1; ++tx) {
+            const int64_t lo = x0 > tx * tw ? x0 : tx * tw, hi = x1 < (tx + 1) * tw ? x1 : (tx + 1) * tw;
+            const int nbits = (int)(hi - lo), shift = (int)(lo - x0);
+            const uint32_t m = (nbits >= 32 ? 0xffffffffu : ((1u << nbits) - 1u)) << shift;
+            long long sum = 0;
+            for (int s = 0; s < nstates; ++s) {
+                uint32_t mt = m;
+                for (int p = 0; p < P; ++p) mt &= ((s >> p) & 1) ? in[p] : ~in[p];
+                sum += vals.v[s] * (long long)__popc(mt);
+            }
+            if (sum) atomicAdd(&acc[ty * 4 + tx], (unsigned long long)sum);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 16 && acc[threadIdx.x]) atomicAdd(&sums[threadIdx.x], acc[threadIdx.x]);
+}
+
+cudaError_t launch_checksum(const grid_geom& g, const uint32_t* planes, const int64_t* values, int nvalues,
+                            unsigned long long* sums, cudaStream_t s) {
+    value_pack vp{};
+    for (int i = 0; i < (1 << kMaxPlanes); ++i) vp.v[i] = i < nvalues ? values[i] : i;
+    checksum_kernel<<<grid_for(g.plane_words, 256), 256, 0, s>>>(planes, g.plane_words, g.wd, g.x_size, g.y_size,
+                                                                 g.planes, vp, sums);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Integer-pipe probe: eight independent chains of three-input logic ops per
+// lane (the same LOP3 class the rule networks compile to).
+// ---------------------------------------------------------------------------
+
+__global__ void lop3_probe_kernel(uint32_t* sink, int iters) {
+    uint32_t r[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) r[i] = threadIdx.x * 0x9E3779B9u + i * 0x85EBCA6Bu + blockIdx.x;
+    const uint32_t a = 0x12345678u ^ blockIdx.x, b = 0x9abcdef0u ^ threadIdx.x;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                asm volatile("lop3.b32 %0, %0, %1, %2, 0x96;" : "+r"(r[i]) : "r"(a), "r"(b ^ (uint32_t)u));
+        }
+    }
+    uint32_t x = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) x ^= r[i];
+    if (x == 0x7fffffffu) sink[0] = x;  // keeps the chains alive
+}
+
+cudaError_t launch_lop3_probe(uint32_t* sink, int blocks, int threads, int iters, cudaStream_t s) {
+    lop3_probe_kernel<<<blocks, threads, 0, s>>>(sink, iters);
+    return cudaGetLastError();
+}
+
+} // namespace cb2

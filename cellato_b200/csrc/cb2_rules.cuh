@@ -1,0 +1,132 @@
+// cb2_rules.cuh -- word-wide rule networks for the bundled automata.
+//
+// Every rule here is a bit-sliced boolean network over 32-bit words: bit i of
+// a word is cell x0+i of one bit-plane (bit b of the cell's state-dictionary
+// index).  The networks are written so that each line is one three-input
+// logic operation (one LOP3 on the GPU).
+//
+// Structure shared by all rules (the "Moore census" shape):
+//   indicator(state)      1 plane: cells equal to the counted state
+//   hagg(l, c, r)         horizontal aggregate of a row's indicator and its
+//                         left/right neighbours (sum as 2 planes, or OR)
+//   next(a, m, b, centre) vertical combine of the aggregates of the rows
+//                         above/at/below plus the centre state -> new state
+// The census includes the centre cell.  That is exact for these rules:
+//   * game of life: with T = live cells in the 3x3 block, next is alive iff
+//     T == 3, or T == 4 and the centre is alive (B3/S23,
+//     game_of_life/algorithm.hpp:36-50);
+//   * wireworld: the head count only matters for a conductor centre, which is
+//     not a head, so the 3x3 count equals the Moore count
+//     (wire/algorithm.hpp:48-59);
+//   * greenberg-hastings: "any excited neighbour" only matters for a
+//     quiescent centre, which is not excited (excitable/algorithm.hpp:58-72).
+// Dictionary indexes follow the reference configs: wire empty=0 head=1 tail=2
+// conductor=3 (wire/config.hpp:21-24); excitable 0..7 (excitable/config.hpp:21-28).
+#pragma once
+
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define CB2_HD __host__ __device__ __forceinline__
+#else
+#define CB2_HD inline
+#endif
+
+namespace cb2 {
+
+// Cell x-1 for every bit of `c`, taking bit 31 of the word to the left.
+CB2_HD uint32_t west_of(uint32_t left, uint32_t c) {
+#if defined(__CUDA_ARCH__)
+    return __funnelshift_l(left, c, 1);
+#else
+    return (c << 1) | (left >> 31);
+#endif
+}
+
+// Cell x+1 for every bit of `c`, taking bit 0 of the word to the right.
+CB2_HD uint32_t east_of(uint32_t c, uint32_t right) {
+#if defined(__CUDA_ARCH__)
+    return __funnelshift_r(c, right, 1);
+#else
+    return (c >> 1) | (right << 31);
+#endif
+}
+
+CB2_HD uint32_t xor3(uint32_t a, uint32_t b, uint32_t c) { return a ^ b ^ c; }
+CB2_HD uint32_t maj3(uint32_t a, uint32_t b, uint32_t c) { return (a & b) | (c & (a | b)); }
+
+// 3x3 census as a bit-sliced sum of three 2-bit row sums (a, m, b), each
+// 0..3.  Returns the low three bits of the total (0..9); bit 3 is never
+// needed by the rules below (see each rule).
+CB2_HD void census_sum(const uint32_t (&a)[2], const uint32_t (&m)[2], const uint32_t (&b)[2], uint32_t& t0,
+                       uint32_t& t1, uint32_t& t2) {
+    t0 = xor3(a[0], m[0], b[0]);
+    uint32_t k0 = maj3(a[0], m[0], b[0]);  // carry into weight 2
+    uint32_t x = xor3(a[1], m[1], b[1]);
+    uint32_t y = maj3(a[1], m[1], b[1]);   // weight 4
+    t1 = x ^ k0;
+    t2 = y ^ (x & k0);
+}
+
+// Game of Life, P = 1 (dead=0, alive=1).
+struct game_of_life {
+    static constexpr int P = 1;   // bit-planes of state
+    static constexpr int NH = 2;  // planes of the horizontal aggregate
+    static constexpr int id = 0;
+    CB2_HD static uint32_t indicator(const uint32_t (&s)[P]) { return s[0]; }
+    CB2_HD static void hagg(uint32_t l, uint32_t c, uint32_t r, uint32_t (&h)[NH]) {
+        h[0] = xor3(l, c, r);
+        h[1] = maj3(l, c, r);
+    }
+    // T == 3 -> alive; T == 4 -> keep centre; otherwise dead.  T <= 9, and the
+    // dropped bit 3 cannot alias 3 (11) or 4 (12).
+    CB2_HD static void next(const uint32_t (&a)[NH], const uint32_t (&m)[NH], const uint32_t (&b)[NH],
+                            const uint32_t (&c)[P], uint32_t (&o)[P]) {
+        uint32_t t0, t1, t2;
+        census_sum(a, m, b, t0, t1, t2);
+        uint32_t e = ~(t0 ^ t1) & (t0 ^ t2);  // (t0,t1,t2) is (1,1,0) or (0,0,1)
+        o[0] = e & (t0 | c[0]);
+    }
+};
+
+// WireWorld, P = 2 (empty=0, head=1, tail=2, conductor=3).
+struct wire {
+    static constexpr int P = 2;
+    static constexpr int NH = 2;
+    static constexpr int id = 1;
+    CB2_HD static uint32_t indicator(const uint32_t (&s)[P]) { return s[0] & ~s[1]; }  // head
+    CB2_HD static void hagg(uint32_t l, uint32_t c, uint32_t r, uint32_t (&h)[NH]) {
+        h[0] = xor3(l, c, r);
+        h[1] = maj3(l, c, r);
+    }
+    // head->tail, tail->conductor, conductor->head iff 1..2 head neighbours,
+    // empty->empty.  A conductor centre has T <= 8, so bit 3 cannot alias 1/2.
+    CB2_HD static void next(const uint32_t (&a)[NH], const uint32_t (&m)[NH], const uint32_t (&b)[NH],
+                            const uint32_t (&c)[P], uint32_t (&o)[P]) {
+        uint32_t t0, t1, t2;
+        census_sum(a, m, b, t0, t1, t2);
+        uint32_t one_or_two = (t0 ^ t1) & ~t2;
+        o[0] = c[1];
+        o[1] = (c[0] ^ c[1]) | (c[0] & c[1] & ~one_or_two);
+    }
+};
+
+// Greenberg-Hastings excitable medium, P = 3 (quiescent=0, excited=1,
+// refractory 2..7).
+struct excitable {
+    static constexpr int P = 3;
+    static constexpr int NH = 1;
+    static constexpr int id = 2;
+    CB2_HD static uint32_t indicator(const uint32_t (&s)[P]) { return s[0] & ~s[1] & ~s[2]; }  // excited
+    CB2_HD static void hagg(uint32_t l, uint32_t c, uint32_t r, uint32_t (&h)[NH]) { h[0] = l | c | r; }
+    // 0 -> 1 iff any excited neighbour; s -> s+1 for 1..6; 7 -> 0.
+    CB2_HD static void next(const uint32_t (&a)[NH], const uint32_t (&m)[NH], const uint32_t (&b)[NH],
+                            const uint32_t (&c)[P], uint32_t (&o)[P]) {
+        uint32_t any = a[0] | m[0] | b[0];
+        o[0] = ~c[0] & (c[1] | c[2] | any);
+        o[1] = c[1] ^ c[0];
+        o[2] = c[2] ^ (c[1] & c[0]);
+    }
+};
+
+} // namespace cb2

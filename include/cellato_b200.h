@@ -1,0 +1,159 @@
+/*
+ * cellato_b200.h -- C-ABI of the B200 (sm_100a) bit-plane traverser backend
+ * for Cellato.
+ *
+ * Plain C types only: device and host memory are `void*`, sizes are
+ * `int64_t`/`size_t`, a CUDA stream is passed as `void*` (a cudaStream_t,
+ * NULL = the legacy default stream, which is what the reference's traversers
+ * launch on: traversers/cuda/simple.cuh:66-67).
+ *
+ * Every function returns CB2_OK (0) or a negative CB2_E* code; the message of
+ * the last failure on the calling thread is available from cb2_last_error().
+ * This replaces the reference's exception convention (CUCH -> CudaError,
+ * traversers/cuda_utils.cuh:37-47; std::runtime_error / std::invalid_argument
+ * for invalid configurations, traversers/cuda/temporal.hpp:57-83): the C++
+ * wrapper in cellato_b200/traverser.hpp rethrows those types.
+ *
+ * Cells, layouts and words follow the reference exactly:
+ *   - a cell's value is its state-dictionary index
+ *     (memory/state_dictionary.hpp:10-42);
+ *   - CB2_LAYOUT_BIT_PLANES is memory/bit_planes_grid.hpp:234-270: P planes,
+ *     each y rows of x/W words, bit i of word xw = cell xw*W + i;
+ *   - CB2_LAYOUT_BIT_ARRAY is memory/bit_array_grid.hpp:80-333;
+ *   - CB2_LAYOUT_TILED_BIT_PLANES is memory/tiled_bit_planes_grid.hpp:35-290;
+ *   - CB2_LAYOUT_STANDARD is one cell per 1 or 4 bytes, row-major
+ *     (memory/standard_grid.hpp:36-60).
+ * Boundaries are toroidal on all four edges (memory/interface.hpp:31-36).
+ */
+#ifndef CELLATO_B200_H
+#define CELLATO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CB2_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------- */
+#define CB2_OK 0
+#define CB2_EINVAL (-1)      /* invalid argument or unsupported configuration */
+#define CB2_ECUDA (-2)       /* a CUDA runtime call failed                    */
+#define CB2_ENOMEM (-3)      /* device memory or the memory budget exhausted  */
+#define CB2_ESTATE (-4)      /* a cell value outside the state dictionary     */
+#define CB2_ETIMEOUT (-5)    /* a bounded device-side wait gave up            */
+#define CB2_ENOTFOUND (-6)   /* unknown request / automaton                    */
+
+/* ---- layouts (experiments/test_suites.hpp:39-125) ------------------------ */
+#define CB2_LAYOUT_STANDARD 0
+#define CB2_LAYOUT_BIT_ARRAY 1
+#define CB2_LAYOUT_BIT_PLANES 2
+#define CB2_LAYOUT_TILED_BIT_PLANES 3
+
+/* ---- bundled automata (src/automata/registry.hpp:17-27) ----------------- */
+#define CB2_GAME_OF_LIFE 0 /* "game-of-life", P=1 (game_of_life/config.hpp)   */
+#define CB2_WIRE 1         /* "wire", P=2 (wire/config.hpp)                    */
+#define CB2_EXCITABLE 2    /* "excitable", P=3 (excitable/config.hpp)          */
+
+int cb2_abi_version(void);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* cb2_last_error(void);
+
+/* Automaton registry.  Replaces the compile-time catalog lookup by name
+ * (suite::is_for, experiments/test_suites.hpp:190-195).  Returns the id or
+ * CB2_ENOTFOUND. */
+int cb2_automaton_lookup(const char* name);
+/* name, bit-planes P and number of states of automaton `id`. */
+int cb2_automaton_info(int id, const char** name, int* planes, int* states);
+
+/* ---- tuning ------------------------------------------------------------- */
+/* Knobs of one run; 0 in any field means "choose automatically" (autotuned
+ * entry if one is cached for this automaton and size, else a heuristic).
+ * Replaces --temporal_steps / --temporal_tile_size_y / --cuda_block_size_*
+ * (experiments/run_params.hpp:10-43). */
+typedef struct cb2_tuning {
+    int temporal_steps; /* generations per HBM round trip: 1, 2, 4 or 8     */
+    int tile_rows;      /* output rows per warp strip                       */
+    int words_per_lane; /* 32-bit words per lane: 1 or 2                    */
+} cb2_tuning;
+
+/* ---- caller-owned device planes ----------------------------------------- */
+/* Advances a grid held in caller-owned device memory, the way a reference
+ * traverser's run(steps) does (traversers/cuda/simple.cuh:44-79,
+ * temporal.cuh:153-245): `a` holds the input planes (P pointers, each
+ * y_size * x_size/32 32-bit words, laid out as CB2_LAYOUT_BIT_PLANES), `b` is
+ * the second buffer of the double buffer.  The two buffers alternate; on
+ * return *result_in_b says which one holds generation `steps`.  x_size must
+ * be a multiple of 32.  Launches only; nothing is synchronised. */
+int cb2_run_bit_planes(int automaton, void* const* a, void* const* b, int64_t x_size, int64_t y_size, int64_t steps,
+                       const cb2_tuning* tuning, void* stream, int* result_in_b);
+
+/* ---- owning device grids -------------------------------------------------- */
+/* A device-resident grid: P bit-planes, double-buffered, generation counter.
+ * Mirrors grid::to_cuda / to_cpu / free_cuda_memory of the reference layouts
+ * (memory/bit_planes_grid.hpp:146-190) plus traverser::init / run /
+ * fetch_result (traversers/cuda/simple.hpp:25-104). */
+typedef struct cb2_grid cb2_grid;
+
+/* x_size must be a multiple of 32 (the 32-bit word of the device layout). */
+int cb2_grid_create(int automaton, int64_t x_size, int64_t y_size, cb2_grid** out);
+int cb2_grid_destroy(cb2_grid* grid);
+
+/* Host image <-> device planes.  `host` may be pageable or pinned memory;
+ * `bytes` must equal cb2_layout_bytes(...).  word_bits: 32 or 64 for the
+ * packed layouts, 8 or 32 (bytes per cell x 8) for CB2_LAYOUT_STANDARD.
+ * Upload returns CB2_ESTATE if a standard-layout cell is not a dictionary
+ * index.  Both calls complete the copy before returning. */
+int cb2_grid_upload(cb2_grid* grid, int layout, int word_bits, const void* host, size_t bytes, void* stream);
+int cb2_grid_download(cb2_grid* grid, int layout, int word_bits, void* host, size_t bytes, void* stream);
+/* Size of a layout's host image for a grid of this automaton and size. */
+int64_t cb2_layout_bytes(int automaton, int layout, int word_bits, int64_t x_size, int64_t y_size);
+
+/* Seeded input on the device: cell i = y*x_size + x draws
+ * u = SplitMix64(seed + (i+1)*0x9E3779B97F4A7C15) >> 11 and takes state
+ * index #{j : thresholds[j] <= u}; thresholds are cumulative probabilities
+ * times 2^53 (at most 7). */
+int cb2_grid_fill_random(cb2_grid* grid, uint64_t seed, const uint64_t* thresholds, int n_thresholds, void* stream);
+
+/* Advances the grid `steps` generations (asynchronous on `stream`). */
+int cb2_grid_run(cb2_grid* grid, int64_t steps, const cb2_tuning* tuning, void* stream);
+
+/* 16-number checksum of the current generation
+ * (memory/standard_grid.hpp:182-218).  state_values maps dictionary index ->
+ * enum value (NULL = identity).  Synchronises `stream`. */
+int cb2_grid_checksum(cb2_grid* grid, const int64_t* state_values, int n_values, uint64_t out[16], void* stream);
+
+/* Device pointers of the current generation's planes (like grid::data()). */
+int cb2_grid_planes(cb2_grid* grid, void** planes, int* n_planes, int64_t* words_per_plane);
+/* Generations advanced since the last upload / fill. */
+int64_t cb2_grid_time_step(const cb2_grid* grid);
+
+/* ---- tuning and measurement --------------------------------------------- */
+/* Times the candidate plans for this automaton and size on the current
+ * device, stores the fastest in the in-process tuning table (used whenever a
+ * cb2_tuning field is 0) and returns it in *best.  `budget_ms` bounds the
+ * time spent (<= 0: a default). */
+int cb2_autotune(int automaton, int64_t x_size, int64_t y_size, double budget_ms, cb2_tuning* best);
+/* Loads / saves the tuning table as text lines
+ * "automaton x_size y_size temporal_steps tile_rows words_per_lane". */
+int cb2_tuning_load(const char* path);
+int cb2_tuning_save(const char* path);
+/* The plan cb2_grid_run would use for a chunk of `steps` generations. */
+int cb2_plan(int automaton, int64_t x_size, int64_t y_size, const cb2_tuning* tuning, cb2_tuning* plan);
+
+/* Measured peak of 32-bit three-input logic ops on the current device
+ * (ops/s), the integer roof of the rule networks. */
+int cb2_measure_lop3_peak(double* ops_per_second);
+
+/* Logic, shift and shuffle instructions the strip kernel issues per 32-bit
+ * word per generation for this automaton (the integer cost of the network). */
+int cb2_network_ops(int automaton, double* alu_ops_per_word, double* shuffles_per_word);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* CELLATO_B200_H */

@@ -1,0 +1,215 @@
+"""ctypes access to the test-only checkers.  TEST INFRASTRUCTURE ONLY.
+
+Only the test suite, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may import this module; the product package never does.
+
+* ``libcellato_oracle.so`` -- the C restatement of Cellato's hot path
+  (``cellato_oracle.c``), each function citing the reference file it follows.
+* ``_ref/libcellato_ref.so`` -- Cellato's own CPU traverser compiled from the
+  reference headers (``ref_shim.cpp``); present wherever ``make -C oracle``
+  ran with the reference sources available, and shipped prebuilt otherwise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from fractions import Fraction
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(_HERE, "libcellato_oracle.so")
+REF_SO = os.path.join(_HERE, "_ref", "libcellato_ref.so")
+
+AUTOMATA = {"game-of-life": 0, "wire": 1, "excitable": 2}
+PLANES = {0: 1, 1: 2, 2: 3}
+LAYOUTS = {"standard": 0, "bit_array": 1, "bit_planes": 2, "tiled_bit_planes": 3}
+
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_i64 = ctypes.c_int64
+
+_oracle = None
+_ref = None
+
+
+def build() -> None:
+    """Compile the checkers (the reference shim only where its sources exist)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def _lib():
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_SO):
+            build()
+        lib = ctypes.CDLL(ORACLE_SO)
+        lib.orc_planes.argtypes = [ctypes.c_int]
+        lib.orc_splitmix64.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
+        lib.orc_splitmix64.restype = ctypes.c_uint64
+        lib.orc_init_cells.argtypes = [_u8p, ctypes.c_uint64, ctypes.c_uint64, _u64p, ctypes.c_int]
+        lib.orc_step_standard.argtypes = [ctypes.c_int, _i64, _i64, _u8p, _u8p]
+        lib.orc_run_standard.argtypes = [ctypes.c_int, _i64, _i64, _i64, _u8p]
+        lib.orc_step_bit_planes.argtypes = [ctypes.c_int, _i64, _i64, _u32p, _u32p]
+        lib.orc_run_bit_planes.argtypes = [ctypes.c_int, _i64, _i64, _i64, _u32p]
+        lib.orc_checksum.argtypes = [_u8p, _i64, _i64, _i64p, _u64p]
+        for name in ("orc_pack_bit_planes", "orc_unpack_bit_planes"):
+            getattr(lib, name).argtypes = [_u8p, _i64, _i64, ctypes.c_int, _u8p]
+        for name in ("orc_pack_bit_array", "orc_unpack_bit_array", "orc_pack_tiled", "orc_unpack_tiled"):
+            getattr(lib, name).argtypes = [_u8p, _i64, _i64, ctypes.c_int, ctypes.c_int, _u8p]
+        _oracle = lib
+    return _oracle
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def _reflib():
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            raise FileNotFoundError(f"{REF_SO} is not built (run `make -C oracle` where the reference sources exist)")
+        lib = ctypes.CDLL(REF_SO)
+        lib.ref_run.argtypes = [ctypes.c_int] * 6 + [_u8p, _u8p, ctypes.c_char_p, ctypes.c_int]
+        lib.ref_pack.argtypes = [ctypes.c_int] * 5 + [_u8p, _u8p, ctypes.c_size_t]
+        lib.ref_bench.argtypes = [ctypes.c_int] * 7 + [_u8p]
+        lib.ref_bench.restype = ctypes.c_double
+        _ref = lib
+    return _ref
+
+
+def _p(a: np.ndarray, t):
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(t)
+
+
+def thresholds(probs) -> np.ndarray:
+    """Cumulative state probabilities (dictionary-index order) as exact 53-bit integer thresholds."""
+    fr = [Fraction(str(p)) if not isinstance(p, Fraction) else p for p in probs]
+    total = sum(fr)
+    if total != 1:
+        raise ValueError(f"probabilities sum to {total}, not 1")
+    out, cum = [], Fraction(0)
+    for p in fr[:-1]:
+        cum += p
+        out.append(int(cum * (1 << 53)))
+    return np.array(out, dtype=np.uint64)
+
+
+def init_cells(x: int, y: int, seed: int, thr: np.ndarray) -> np.ndarray:
+    cells = np.empty(x * y, dtype=np.uint8)
+    thr = np.ascontiguousarray(thr, dtype=np.uint64)
+    _lib().orc_init_cells(_p(cells, _u8p), x * y, seed, _p(thr, _u64p), len(thr))
+    return cells.reshape(y, x)
+
+
+def splitmix64(seed: int, index: int) -> int:
+    return int(_lib().orc_splitmix64(seed, index))
+
+
+def run_standard(automaton: int, cells: np.ndarray, steps: int) -> np.ndarray:
+    c = np.ascontiguousarray(cells, dtype=np.uint8).copy()
+    y, x = c.shape
+    rc = _lib().orc_run_standard(automaton, x, y, steps, _p(c, _u8p))
+    if rc:
+        raise ValueError(f"orc_run_standard failed ({rc})")
+    return c
+
+
+def run_bit_planes(automaton: int, planes: np.ndarray, x: int, y: int, steps: int) -> np.ndarray:
+    """planes: uint32 array of P*y*(x/32) words (plane-major)."""
+    p = np.ascontiguousarray(planes, dtype=np.uint32).copy()
+    rc = _lib().orc_run_bit_planes(automaton, x, y, steps, _p(p, _u32p))
+    if rc:
+        raise ValueError(f"orc_run_bit_planes failed ({rc})")
+    return p
+
+
+def checksum(cells: np.ndarray, values=None) -> list[int]:
+    c = np.ascontiguousarray(cells, dtype=np.uint8)
+    y, x = c.shape
+    vals = np.arange(256, dtype=np.int64) if values is None else np.ascontiguousarray(values, dtype=np.int64)
+    out = np.zeros(16, dtype=np.uint64)
+    _lib().orc_checksum(_p(c, _u8p), x, y, _p(vals, _i64p), _p(out, _u64p))
+    return [int(v) for v in out]
+
+
+def checksum_str(cells: np.ndarray, values=None) -> str:
+    return "-".join(str(v) for v in checksum(cells, values))
+
+
+def pack(layout: str, cells: np.ndarray, planes: int, word_bits: int) -> np.ndarray:
+    c = np.ascontiguousarray(cells, dtype=np.uint8)
+    y, x = c.shape
+    lib = _lib()
+    if layout == "bit_planes":
+        out = np.zeros(planes * y * x // 8, dtype=np.uint8)
+        rc = lib.orc_pack_bit_planes(_p(c, _u8p), x, y, planes, _p(out, _u8p))
+    elif layout == "bit_array":
+        cpw = word_bits // planes
+        out = np.zeros((x * y // cpw) * (word_bits // 8), dtype=np.uint8)
+        rc = lib.orc_pack_bit_array(_p(c, _u8p), x, y, planes, word_bits, _p(out, _u8p))
+    elif layout == "tiled_bit_planes":
+        out = np.zeros(planes * y * x // 8, dtype=np.uint8)
+        rc = lib.orc_pack_tiled(_p(c, _u8p), x, y, planes, word_bits, _p(out, _u8p))
+    else:
+        raise ValueError(layout)
+    if rc:
+        raise ValueError(f"pack {layout} failed ({rc})")
+    return out
+
+
+def unpack(layout: str, data: np.ndarray, x: int, y: int, planes: int, word_bits: int) -> np.ndarray:
+    d = np.ascontiguousarray(data).view(np.uint8)
+    cells = np.empty((y, x), dtype=np.uint8)
+    lib = _lib()
+    if layout == "bit_planes":
+        rc = lib.orc_unpack_bit_planes(_p(d, _u8p), x, y, planes, _p(cells, _u8p))
+    elif layout == "bit_array":
+        rc = lib.orc_unpack_bit_array(_p(d, _u8p), x, y, planes, word_bits, _p(cells, _u8p))
+    elif layout == "tiled_bit_planes":
+        rc = lib.orc_unpack_tiled(_p(d, _u8p), x, y, planes, word_bits, _p(cells, _u8p))
+    else:
+        raise ValueError(layout)
+    if rc:
+        raise ValueError(f"unpack {layout} failed ({rc})")
+    return cells
+
+
+# ---- the reference itself (oracle/_ref) ------------------------------------------------------
+
+def ref_run(automaton: int, cells: np.ndarray, steps: int, layout: str = "standard", word_bits: int = 64):
+    """Reference CPU simple traverser; returns (final cells, checksum string)."""
+    c = np.ascontiguousarray(cells, dtype=np.uint8)
+    y, x = c.shape
+    out = np.empty_like(c)
+    buf = ctypes.create_string_buffer(1024)
+    rc = _reflib().ref_run(automaton, LAYOUTS[layout], word_bits, x, y, steps, _p(c, _u8p), _p(out, _u8p), buf, 1024)
+    if rc:
+        raise ValueError(f"ref_run failed ({rc})")
+    return out, buf.value.decode()
+
+
+def ref_pack(automaton: int, layout: str, cells: np.ndarray, word_bits: int) -> np.ndarray:
+    c = np.ascontiguousarray(cells, dtype=np.uint8)
+    y, x = c.shape
+    out = np.zeros(x * y, dtype=np.uint8)  # packed layouts never exceed one byte per cell
+    n = _reflib().ref_pack(automaton, LAYOUTS[layout], word_bits, x, y, _p(c, _u8p), _p(out, _u8p), out.nbytes)
+    if n < 0:
+        raise ValueError(f"ref_pack failed ({n})")
+    return out[:n].copy()
+
+
+def ref_bench(automaton: int, cells: np.ndarray, steps: int, threads: int, layout: str = "bit_planes",
+              word_bits: int = 64) -> float:
+    """Seconds taken by the slowest of `threads` independent reference traversers."""
+    c = np.ascontiguousarray(cells, dtype=np.uint8)
+    y, x = c.shape
+    s = _reflib().ref_bench(automaton, LAYOUTS[layout], word_bits, x, y, steps, threads, _p(c, _u8p))
+    if s < 0:
+        raise RuntimeError("ref_bench failed")
+    return float(s)

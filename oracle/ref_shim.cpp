@@ -1,0 +1,223 @@
+// ref_shim.cpp -- TEST INFRASTRUCTURE ONLY.
+//
+// A small C-ABI driver around Cellato's OWN CPU path, compiled straight from
+// the reference headers by oracle/Makefile into oracle/_ref/libcellato_ref.so.
+// It is the checker for the C restatement in cellato_oracle.c, the generator
+// of the committed golden fixtures, and the CPU arm of the benchmark
+// ("reference" kind).  The product library never links or loads it.
+//
+// It follows experiment_manager::run_round (experiments/experiment_manager.hpp:64-93):
+// build a standard grid from the caller's cells, convert it to the suite's
+// layout, init + run the CPU simple traverser (traversers/cpu/simple.hpp:19-95),
+// fetch_result().to_standard(), and read get_checksum()
+// (memory/standard_grid.hpp:182-218).  Cells cross the ABI as uint8 state
+// dictionary indexes (memory/state_dictionary.hpp:10-42).
+
+#include <atomic>
+#include <chrono>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "cellato/experiments/run_params.hpp"
+#include "cellato/experiments/test_suites.hpp"
+
+#include "excitable/config.hpp"
+#include "game_of_life/config.hpp"
+#include "wire/config.hpp"
+
+namespace {
+
+namespace ts = cellato::run::test_suites;
+
+enum layout_id { L_STANDARD = 0, L_BIT_ARRAY = 1, L_BIT_PLANES = 2, L_TILED = 3 };
+
+template <typename suite>
+int run_suite(int x, int y, int steps, const uint8_t* in, uint8_t* out, char* checksum, int checksum_len) {
+    using automaton = typename suite::automaton;
+    using dict = typename automaton::state_dictionary;
+    using cell_t = typename suite::original_cell_t;
+    using grid_t = typename suite::grid_t;
+    using traverser_t = typename suite::traverser_t;
+
+    cellato::run::run_params params;
+    params.x_size = x;
+    params.y_size = y;
+    params.steps = steps;
+
+    cellato::memory::grids::standard::grid<cell_t> initial(x, y);
+    cell_t* data = initial.data();
+    for (std::size_t i = 0; i < (std::size_t)x * (std::size_t)y; ++i) data[i] = dict::index_to_state(in[i]);
+
+    grid_t grid = initial;
+    traverser_t traverser;
+    traverser.init(grid, params);
+    traverser.run(steps);
+    grid_t result = traverser.fetch_result();
+    auto standard = result.to_standard();
+
+    if (out) {
+        const cell_t* res = standard.data();
+        for (std::size_t i = 0; i < (std::size_t)x * (std::size_t)y; ++i) out[i] = (uint8_t)dict::state_to_index(res[i]);
+    }
+    if (checksum && checksum_len > 0) {
+        std::string c = standard.get_checksum();
+        std::strncpy(checksum, c.c_str(), (std::size_t)checksum_len - 1);
+        checksum[checksum_len - 1] = '\0';
+    }
+    return 0;
+}
+
+template <typename automaton, typename fn_t>
+int with_suite(int layout, int word_bits, fn_t&& fn) {
+    switch (layout) {
+    case L_STANDARD: return fn.template operator()<ts::on_cpu::standard<automaton>>();
+    case L_BIT_ARRAY:
+        if (word_bits == 32) return fn.template operator()<ts::on_cpu::using_<std::uint32_t>::bit_array<automaton>>();
+        if (word_bits == 64) return fn.template operator()<ts::on_cpu::using_<std::uint64_t>::bit_array<automaton>>();
+        return -3;
+    case L_BIT_PLANES:
+        if (word_bits == 32) return fn.template operator()<ts::on_cpu::using_<std::uint32_t>::bit_planes<automaton>>();
+        if (word_bits == 64) return fn.template operator()<ts::on_cpu::using_<std::uint64_t>::bit_planes<automaton>>();
+        return -3;
+    case L_TILED:
+        if (word_bits == 32)
+            return fn.template operator()<ts::on_cpu::using_<std::uint32_t>::tiled_bit_planes<automaton>>();
+        if (word_bits == 64)
+            return fn.template operator()<ts::on_cpu::using_<std::uint64_t>::tiled_bit_planes<automaton>>();
+        return -3;
+    default: return -2;
+    }
+}
+
+template <typename fn_t>
+int with_automaton(int automaton, int layout, int word_bits, fn_t&& fn) {
+    switch (automaton) {
+    case 0: return with_suite<game_of_life::config>(layout, word_bits, fn);
+    case 1: return with_suite<wire::config>(layout, word_bits, fn);
+    case 2: return with_suite<excitable::config>(layout, word_bits, fn);
+    default: return -1;
+    }
+}
+
+// The layout's host words, exactly as the reference grid stores them.
+template <typename suite>
+int pack_suite(int x, int y, const uint8_t* in, uint8_t* out, std::size_t out_len) {
+    using automaton = typename suite::automaton;
+    using dict = typename automaton::state_dictionary;
+    using cell_t = typename suite::original_cell_t;
+    using grid_t = typename suite::grid_t;
+
+    cellato::memory::grids::standard::grid<cell_t> initial(x, y);
+    cell_t* data = initial.data();
+    for (std::size_t i = 0; i < (std::size_t)x * (std::size_t)y; ++i) data[i] = dict::index_to_state(in[i]);
+    grid_t grid = initial;
+    std::size_t written = 0;
+    if constexpr (requires { grid.raw_data(); }) {
+        using word_t = typename grid_t::store_type;
+        std::size_t words = (std::size_t)x * (std::size_t)y / grid_t::cells_per_word;
+        std::size_t bytes = words * sizeof(word_t);
+        if (bytes > out_len) return -4;
+        std::memcpy(out, grid.raw_data(), bytes);
+        written = bytes;
+    } else if constexpr (requires { grid.data().size(); }) {
+        using word_t = typename grid_t::store_type;
+        auto planes = grid.data();
+        std::size_t words = grid.x_size_physical() * grid.y_size_physical();
+        for (std::size_t p = 0; p < planes.size(); ++p) {
+            if (written + words * sizeof(word_t) > out_len) return -4;
+            std::memcpy(out + written, planes[p], words * sizeof(word_t));
+            written += words * sizeof(word_t);
+        }
+    } else {
+        return -2; // the standard layout has no packed words
+    }
+    return (int)written;
+}
+
+} // namespace
+
+extern "C" {
+
+// Runs `steps` generations of the reference CPU simple traverser with the
+// requested layout (0 standard, 1 bit_array, 2 bit_planes, 3 tiled) and word
+// size.  in/out hold x*y dictionary indexes; out and checksum may be null.
+int ref_run(int automaton, int layout, int word_bits, int x, int y, int steps, const uint8_t* in, uint8_t* out,
+            char* checksum, int checksum_len) {
+    try {
+        return with_automaton(automaton, layout, word_bits, [&]<typename suite>() {
+            return run_suite<suite>(x, y, steps, in, out, checksum, checksum_len);
+        });
+    } catch (...) {
+        return -10;
+    }
+}
+
+// Host byte image of the layout's grid words (bit_array, bit_planes, tiled).
+int ref_pack(int automaton, int layout, int word_bits, int x, int y, const uint8_t* in, uint8_t* out, size_t out_len) {
+    if (layout == L_STANDARD) return -2;
+    try {
+        return with_automaton(automaton, layout, word_bits, [&]<typename suite>() {
+            return pack_suite<suite>(x, y, in, out, out_len);
+        });
+    } catch (...) {
+        return -10;
+    }
+}
+
+// Throughput sample for the CPU baseline: `threads` host threads each run an
+// independent copy of the reference traverser on the same x*y input for
+// `steps` generations.  Returns the wall time of the slowest thread in
+// seconds (the traversers' init and fetch are outside the timed region), or
+// a negative value on error.
+double ref_bench(int automaton, int layout, int word_bits, int x, int y, int steps, int threads, const uint8_t* in) {
+    if (threads < 1) threads = 1;
+    std::vector<double> secs((std::size_t)threads, -1.0);
+    std::atomic<int> ready{0};
+    auto body = [&](int t) {
+        try {
+            with_automaton(automaton, layout, word_bits, [&]<typename suite>() {
+                using automaton_t = typename suite::automaton;
+                using dict = typename automaton_t::state_dictionary;
+                using cell_t = typename suite::original_cell_t;
+                using grid_t = typename suite::grid_t;
+                using traverser_t = typename suite::traverser_t;
+                cellato::run::run_params params;
+                params.x_size = x;
+                params.y_size = y;
+                params.steps = steps;
+                cellato::memory::grids::standard::grid<cell_t> initial(x, y);
+                cell_t* data = initial.data();
+                for (std::size_t i = 0; i < (std::size_t)x * (std::size_t)y; ++i)
+                    data[i] = dict::index_to_state(in[i]);
+                grid_t grid = initial;
+                traverser_t traverser;
+                traverser.init(grid, params);
+                ready.fetch_add(1);
+                while (ready.load() < threads) std::this_thread::yield();
+                auto t0 = std::chrono::steady_clock::now();
+                traverser.run(steps);
+                auto t1 = std::chrono::steady_clock::now();
+                secs[(std::size_t)t] = std::chrono::duration<double>(t1 - t0).count();
+                grid_t result = traverser.fetch_result();
+                (void)result;
+                return 0;
+            });
+        } catch (...) {
+            ready.fetch_add(1);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t) pool.emplace_back(body, t);
+    for (auto& th : pool) th.join();
+    double worst = 0;
+    for (double s : secs) {
+        if (s < 0) return -1.0;
+        worst = s > worst ? s : worst;
+    }
+    return worst;
+}
+
+} // extern "C"

@@ -1,0 +1,74 @@
+"""The oracle (oracle/cellato_oracle.c) pinned against Cellato itself: the
+golden fixtures produced by the reference build, and -- where the reference
+build is present -- direct runs of the reference CPU traverser."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.golden.make_golden import unpack_cells
+
+
+def test_generator_matches_golden(golden):
+    cases, arrays = golden
+    for c in cases:
+        cells = O.init_cells(c["x"], c["y"], c["seed"], np.array(c["thresholds"], dtype=np.uint64))
+        assert O.checksum_str(cells) == c["initial_checksum"]
+        if "cells" in c:
+            want = unpack_cells(arrays[c["cells"] + "_init"], c["automaton"], c["x"], c["y"])
+            assert (cells == want).all()
+
+
+def test_thresholds_are_exact():
+    assert list(O.thresholds([0.5, 0.5])) == [1 << 52]
+    assert list(O.thresholds([0.125] * 8)) == [i << 50 for i in range(1, 8)]
+    with pytest.raises(ValueError):
+        O.thresholds([0.5, 0.6])
+
+
+@pytest.mark.parametrize("stepper", ["standard", "bit_planes"])
+def test_oracle_matches_golden(golden, stepper):
+    cases, arrays = golden
+    for c in cases:
+        if stepper == "standard" and c["x"] * c["y"] * c["steps"] > 2e7:
+            continue
+        a, x, y = c["automaton"], c["x"], c["y"]
+        cells = O.init_cells(x, y, c["seed"], np.array(c["thresholds"], dtype=np.uint64))
+        if stepper == "standard":
+            out = O.run_standard(a, cells, c["steps"])
+        else:
+            P = O.PLANES[a]
+            planes = O.pack("bit_planes", cells, P, 32).view(np.uint32)
+            out = O.unpack("bit_planes", O.run_bit_planes(a, planes, x, y, c["steps"]), x, y, P, 32)
+        assert O.checksum_str(out) == c["checksum"], (c, stepper)
+        if "cells" in c:
+            assert (out == unpack_cells(arrays[c["cells"] + "_out"], a, x, y)).all()
+
+
+def test_checksum_tiles_ragged():
+    # 4x4 tiles of ceil(X/4) x ceil(Y/4); the last tile row/column may be short or empty.
+    cells = np.ones((5, 32), dtype=np.uint8)
+    ck = O.checksum(cells)
+    assert ck == [16, 16, 16, 16] * 2 + [8, 8, 8, 8] + [0, 0, 0, 0]
+    vals = np.arange(256, dtype=np.int64) * 3
+    assert O.checksum(cells, vals) == [3 * v for v in ck]
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("automaton", [0, 1, 2])
+def test_oracle_matches_reference_all_layouts(automaton):
+    P = O.PLANES[automaton]
+    probs = {0: [0.5, 0.5], 1: [0.6, 0.05, 0.05, 0.3], 2: [0.125] * 8}[automaton]
+    for (x, y, steps, seed) in [(64, 32, 7, 1), (128, 40, 13, 42), (320, 24, 9, 5)]:
+        cells = O.init_cells(x, y, seed, O.thresholds(probs))
+        ref_cells, ref_ck = O.ref_run(automaton, cells, steps)
+        assert (O.run_standard(automaton, cells, steps) == ref_cells).all()
+        for layout in ("bit_planes", "bit_array", "tiled_bit_planes"):
+            for W in (32, 64):
+                if (layout == "bit_array" and x % (W // P)) or (layout == "bit_planes" and x % W) or \
+                        (layout == "tiled_bit_planes" and y % (W // 8)):
+                    continue
+                packed = O.pack(layout, cells, P, W)
+                assert packed.tobytes() == O.ref_pack(automaton, layout, cells, W).tobytes(), (layout, W)
+                assert (O.unpack(layout, packed, x, y, P, W) == cells).all()
+                rc, rck = O.ref_run(automaton, cells, steps, layout, W)
+                assert rck == ref_ck and (rc == ref_cells).all(), (layout, W)
