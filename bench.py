@@ -185,7 +185,9 @@ def traffic_for(kernel_key: str):
 def launches_per_run(gens: int, k: int) -> int:
     n, left = 0, gens
     while left > 0:
-        step = k if left >= k else (4 if left >= 4 else 2 if left >= 2 else 1)
+        step = k
+        while step > left:
+            step //= 2
         left -= step
         n += 1
     return n
@@ -272,7 +274,8 @@ def main() -> None:
     int_gops = int_ops_per_launch / avg_launch_s / 1e9
     int_frac = int_gops / (lop3_peak / 1e9)
     hbm_frac = hbm_gbs / hbm_peak
-    kernel_key = f"strip_kernel<{name},K={k},V={plan['words_per_lane']}>@{x}x{y}"
+    kernel_key = (f"pipe_kernel<{name},K={k},V={plan['words_per_lane']},L={plan['levels_per_warp']}>"
+                  f"@{x}x{y}")
     traffic = traffic_for(kernel_key)
     roof = {
         "bound": "int" if int_frac >= hbm_frac else "hbm",

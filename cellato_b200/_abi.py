@@ -49,11 +49,12 @@ class StateError(ValueError):
 
 
 class Tuning(ctypes.Structure):
-    _fields_ = [("temporal_steps", ctypes.c_int), ("tile_rows", ctypes.c_int), ("words_per_lane", ctypes.c_int)]
+    _fields_ = [("temporal_steps", ctypes.c_int), ("tile_rows", ctypes.c_int), ("words_per_lane", ctypes.c_int),
+                ("levels_per_warp", ctypes.c_int)]
 
     def as_dict(self):
         return {"temporal_steps": self.temporal_steps, "tile_rows": self.tile_rows,
-                "words_per_lane": self.words_per_lane}
+                "words_per_lane": self.words_per_lane, "levels_per_warp": self.levels_per_warp}
 
 
 _i64 = ctypes.c_int64
@@ -138,5 +139,5 @@ def declared_symbols() -> list[str]:
     return sorted(set(re.findall(r"\b(cb2_[a-z0-9_]+)\s*\(", text)))
 
 
-def tuning(temporal_steps: int = 0, tile_rows: int = 0, words_per_lane: int = 0) -> Tuning:
-    return Tuning(temporal_steps, tile_rows, words_per_lane)
+def tuning(temporal_steps: int = 0, tile_rows: int = 0, words_per_lane: int = 0, levels_per_warp: int = 0) -> Tuning:
+    return Tuning(temporal_steps, tile_rows, words_per_lane, levels_per_warp)

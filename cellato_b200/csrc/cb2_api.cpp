@@ -92,24 +92,40 @@ static bool tuned_entry(int automaton, int64_t x, int64_t y, cb2_tuning* out) {
     return false;
 }
 
-static bool valid_k(int k) { return k == 1 || k == 2 || k == 4 || k == 8; }
+static bool valid_k(int k) { return k == 1 || k == 2 || k == 4 || k == 8 || k == 16; }
+
+// Default (K, V, L) per automaton, the fastest plans measured on B200 at the
+// headline sizes; cb2_autotune replaces them per size.
+static const int kDefaultPlan[kNumAutomata][3] = {{8, 2, 4}, {16, 2, 2}, {8, 1, 8}};
 
 // Fills every 0 field of `t` for a grid of geometry g.
 static int resolve_plan(const grid_geom& g, const cb2_tuning* t, run_plan* plan) {
-    cb2_tuning want{0, 0, 0};
+    cb2_tuning want{0, 0, 0, 0};
     if (t) want = *t;
-    cb2_tuning tuned{0, 0, 0};
+    cb2_tuning tuned{0, 0, 0, 0};
     const bool have_tuned = tuned_entry(g.automaton, g.x_size, g.y_size, &tuned);
-    int k = want.temporal_steps ? want.temporal_steps : (have_tuned ? tuned.temporal_steps : 8);
-    int v = want.words_per_lane ? want.words_per_lane : (have_tuned ? tuned.words_per_lane : (g.wd <= 30 ? 1 : 2));
-    if (!valid_k(k)) return fail(CB2_EINVAL, "temporal_steps must be 1, 2, 4 or 8 (got " + std::to_string(k) + ")");
-    if (v != 1 && v != 2) return fail(CB2_EINVAL, "words_per_lane must be 1 or 2 (got " + std::to_string(v) + ")");
+    const int* def = kDefaultPlan[g.automaton];
+    const int k = want.temporal_steps ? want.temporal_steps : (have_tuned ? tuned.temporal_steps : def[0]);
+    if (!valid_k(k)) return fail(CB2_EINVAL, "temporal_steps must be 1, 2, 4, 8 or 16 (got " + std::to_string(k) + ")");
+    const bool tuned_k = have_tuned && tuned.temporal_steps == k;
+    int v = want.words_per_lane;
+    if (!v) v = tuned_k ? tuned.words_per_lane : (g.wd <= 30 ? 1 : (k == def[0] ? def[1] : 2));
+    if (v != 1 && v != 2 && v != 4)
+        return fail(CB2_EINVAL, "words_per_lane must be 1, 2 or 4 (got " + std::to_string(v) + ")");
+    int l = want.levels_per_warp;
+    if (!l) l = (tuned_k && tuned.words_per_lane == v) ? tuned.levels_per_warp : (k == def[0] && v == def[1] ? def[2] : 0);
+    const strip_variant* sv = find_variant(g.automaton, k, v, l);
+    if (!sv && !want.levels_per_warp) sv = find_variant(g.automaton, k, v, 0);
+    if (!sv)
+        return fail(CB2_EINVAL, "no strip kernel for temporal_steps=" + std::to_string(k) + ", words_per_lane=" +
+                                    std::to_string(v) + ", levels_per_warp=" + std::to_string(l));
     int rows = want.tile_rows;
-    if (!rows && have_tuned && tuned.temporal_steps == k && tuned.words_per_lane == v) rows = tuned.tile_rows;
-    if (!rows) rows = auto_tile_rows(g, k, v);
+    if (!rows && tuned_k && tuned.words_per_lane == sv->v && tuned.levels_per_warp == sv->l) rows = tuned.tile_rows;
+    if (!rows) rows = auto_tile_rows(g, *sv);
     if (rows < 1) return fail(CB2_EINVAL, "tile_rows must be positive");
-    plan->k = k;
-    plan->v = v;
+    plan->k = sv->k;
+    plan->v = sv->v;
+    plan->l = sv->l;
     plan->tile_rows = std::min(rows, (int)g.h);
     return CB2_OK;
 }
@@ -140,9 +156,11 @@ static int run_chunks(const grid_geom& g, uint32_t* const bufs[2], int cur, int6
     int64_t left = steps;
     while (left > 0) {
         run_plan p = main_plan;
-        if (left < p.k) {  // remainder in powers of two
-            p.k = left >= 4 ? 4 : left >= 2 ? 2 : 1;
-            cb2_tuning t2{p.k, 0, p.v};
+        if (left < p.k) {  // remainder in powers of two, same lane width where possible
+            int k = 1;
+            while (k * 2 <= left) k *= 2;
+            cb2_tuning t2{k, 0, p.v, 0};
+            if (!find_variant(g.automaton, k, p.v, 0)) t2.words_per_lane = 0;
             rc = resolve_plan(g, &t2, &p);
             if (rc) return rc;
         }
@@ -413,7 +431,7 @@ int cb2_plan(int automaton, int64_t x_size, int64_t y_size, const cb2_tuning* tu
     run_plan p;
     rc = resolve_plan(g, tuning, &p);
     if (rc) return rc;
-    if (plan) *plan = cb2_tuning{p.k, p.tile_rows, p.v};
+    if (plan) *plan = cb2_tuning{p.k, p.tile_rows, p.v, p.l};
     return CB2_OK;
 }
 
@@ -438,21 +456,18 @@ int cb2_autotune(int automaton, int64_t x_size, int64_t y_size, double budget_ms
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     std::vector<cb2_tuning> cands;
-    for (int k : {8, 4, 2, 1})
-        for (int v : {2, 1}) {
-            run_plan base{k, v, auto_tile_rows(g, k, v)};
-            for (int mul : {1, 2, 4}) {
-                int rows = std::min<int>((int)g.h, base.tile_rows * mul);
-                cands.push_back(cb2_tuning{k, rows, v});
-                if (rows == (int)g.h) break;
-            }
-        }
+    for (const strip_variant& sv : strip_variants(automaton)) {
+        if (sv.k < 4) continue;  // one- and two-generation passes are memory-bound at any size
+        const int rows = auto_tile_rows(g, sv);
+        cands.push_back(cb2_tuning{sv.k, rows, sv.v, sv.l});
+        if (rows * 2 <= (int)g.h) cands.push_back(cb2_tuning{sv.k, rows * 2, sv.v, sv.l});
+    }
     double best_ns = 1e300;
     cb2_tuning pick = cands.front();
     double spent = 0;
     for (const cb2_tuning& c : cands) {
         if (spent > budget_ms) break;
-        const int64_t gens = std::max<int64_t>(8, c.temporal_steps * 2);
+        const int64_t gens = 32;  // the same generations for every candidate
         rc = cb2_grid_run(grid, c.temporal_steps, &c, nullptr);  // warm-up
         if (rc) break;
         cudaEventRecord(e0);
@@ -492,11 +507,12 @@ int cb2_tuning_load(const char* path) {
         std::string name;
         long long x, y;
         cb2_tuning t{};
-        if (!(is >> name >> x >> y >> t.temporal_steps >> t.tile_rows >> t.words_per_lane))
+        if (!(is >> name >> x >> y >> t.temporal_steps >> t.tile_rows >> t.words_per_lane >> t.levels_per_warp))
             return fail(CB2_EINVAL, "malformed tuning line: " + line);
         int a = find_automaton(name.c_str());
         if (a < 0) return fail(CB2_ENOTFOUND, "unknown automaton in tuning file: " + name);
-        if (!valid_k(t.temporal_steps) || t.words_per_lane < 1 || t.words_per_lane > 2 || t.tile_rows < 1)
+        if (!valid_k(t.temporal_steps) || !find_variant(a, t.temporal_steps, t.words_per_lane, t.levels_per_warp) ||
+            t.tile_rows < 1)
             return fail(CB2_EINVAL, "invalid tuning values: " + line);
         std::lock_guard<std::mutex> lock(g_tune_mu);
         g_tune[{a, x, y}] = t;
@@ -508,11 +524,12 @@ int cb2_tuning_load(const char* path) {
 int cb2_tuning_save(const char* path) {
     std::ofstream f(path ? path : "");
     if (!f) return fail(CB2_EINVAL, std::string("cannot write tuning file ") + (path ? path : "(null)"));
-    f << "# automaton x_size y_size temporal_steps tile_rows words_per_lane\n";
+    f << "# automaton x_size y_size temporal_steps tile_rows words_per_lane levels_per_warp\n";
     std::lock_guard<std::mutex> lock(g_tune_mu);
     for (auto& kv : g_tune)
         f << kNames[kv.first.automaton] << ' ' << kv.first.x << ' ' << kv.first.y << ' ' << kv.second.temporal_steps
-          << ' ' << kv.second.tile_rows << ' ' << kv.second.words_per_lane << '\n';
+          << ' ' << kv.second.tile_rows << ' ' << kv.second.words_per_lane << ' ' << kv.second.levels_per_warp
+          << '\n';
     return (int)g_tune.size();
 }
 

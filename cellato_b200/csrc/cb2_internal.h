@@ -6,13 +6,14 @@
 
 #include <cstdint>
 #include <string>
+#include <vector>
 
 namespace cb2 {
 
 constexpr int kMaxPlanes = 3;
 constexpr int kNumAutomata = 3;
 constexpr int kMaxThresholds = 7;  // up to 8 states
-constexpr int kStripWarpsPerBlock = 4;
+constexpr int kRingDepth = 8;  // input rows kept in flight per strip task
 
 // Geometry of one device grid: P planes of h rows x wd 32-bit words.
 struct grid_geom {
@@ -25,9 +26,18 @@ struct grid_geom {
 
 // Tuning knobs for one single-grid run.
 struct run_plan {
-    int k;          // generations per launch (1, 2, 4 or 8)
-    int v;          // words per lane (1 or 2)
+    int k;          // generations per launch (1, 2, 4, 8 or 16)
+    int v;          // 32-bit words per lane (1, 2 or 4)
+    int l;          // levels (generations) per warp; the CTA has k / l warps
     int tile_rows;  // output rows per strip task
+};
+
+// One instantiated strip kernel.
+struct strip_variant {
+    int k, v, l;
+    const void* fn;
+    int threads;
+    int smem_bytes;
 };
 
 int planes_of(int automaton);
@@ -37,12 +47,16 @@ int find_automaton(const char* name);
 // Launches one K-generation strip pass over a whole grid (in -> out).
 cudaError_t launch_strip_pass(const grid_geom& g, const uint32_t* in, uint32_t* out, const run_plan& plan,
                               cudaStream_t stream);
-// Strip tasks per column and per row for a plan, and the number of tasks.
+// Strip tasks per column and per row for a plan.
 void strip_counts(const grid_geom& g, int v, int tile_rows, int* nsx, int* nsy);
+// The instantiated kernels of an automaton, and the first one matching a
+// plan (v or l of 0 match anything).
+const std::vector<strip_variant>& strip_variants(int automaton);
+const strip_variant* find_variant(int automaton, int k, int v, int l);
 // Output rows per task so that one launch fills the GPU about once.
-int auto_tile_rows(const grid_geom& g, int k, int v);
-// Registers-limited number of resident strip warps on this device.
-int resident_strip_warps(int automaton, int k, int v);
+int auto_tile_rows(const grid_geom& g, const strip_variant& sv);
+// Number of strip-task CTAs resident at once on this device.
+int resident_strip_tasks(const strip_variant& sv);
 
 // Layout conversions between host images and device planes (device -> device).
 cudaError_t launch_pack_cells(const grid_geom& g, const void* cells, int cell_bytes, uint32_t* planes,

@@ -1,6 +1,6 @@
 // cb2_kernels.cu -- device kernels of the library and their launchers.
 //
-//  * strip_kernel<Rule, K, V>   the hot path (cb2_strip.cuh), K generations
+//  * pipe_kernel<Rule, K, V, L> the hot path (cb2_pipe.cuh), K generations
 //                               per launch over a whole grid
 //  * layout conversion kernels  standard / bit_array / tiled host images to
 //                               and from the device's linear bit planes
@@ -11,16 +11,18 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <map>
 #include <mutex>
+#include <vector>
 
 #include "cb2_internal.h"
 #include "cb2_rules.cuh"
-#include "cb2_strip.cuh"
+#include "cb2_pipe.cuh"
 
 namespace cb2 {
 
 // ---------------------------------------------------------------------------
-// Strip pass
+// Strip pass: one CTA per strip task, K generations per launch
 // ---------------------------------------------------------------------------
 
 struct strip_launch {
@@ -31,12 +33,12 @@ struct strip_launch {
     int32_t nsx, nsy, tile_rows;
 };
 
-template <class R, int K, int V>
-__global__ void __launch_bounds__(kStripWarpsPerBlock * 32) strip_kernel(strip_launch a) {
-    const int warp = blockIdx.x * kStripWarpsPerBlock + (threadIdx.x >> 5);
-    if (warp >= a.nsx * a.nsy) return;  // whole warps only
+template <class R, int K, int V, int L>
+__global__ void __launch_bounds__(32 * (K / L)) pipe_kernel(strip_launch a) {
+    extern __shared__ __align__(16) uint32_t smem[];
     constexpr int own = 32 * V - 2;
-    const int sx = warp % a.nsx, sy = warp / a.nsx;
+    const int task = blockIdx.x;
+    const int sx = task % a.nsx, sy = task / a.nsx;
     strip_task t;
     t.in = a.in;
     t.out = a.out;
@@ -47,33 +49,45 @@ __global__ void __launch_bounds__(kStripWarpsPerBlock * 32) strip_kernel(strip_l
     t.nx = min(own, a.wd - t.x0);
     t.y0 = sy * a.tile_rows;
     t.ny = min(a.tile_rows, a.h - t.y0);
-    strip_run<R, K, V>(t);
+    pipe_run<R, K, V, L, kRingDepth>(t, smem);
 }
 
-using strip_fn = void (*)(strip_launch);
+template <class R, int K, int V, int L>
+static strip_variant make_variant() {
+    return strip_variant{K, V, L, (const void*)pipe_kernel<R, K, V, L>, 32 * (K / L),
+                         4 * pipe_smem_words<R, K, V, L, kRingDepth>()};
+}
 
+// The instantiated (K, V, L) plans; for each (K, V) the first entry is the
+// default levels-per-warp.
 template <class R>
-static strip_fn strip_for(int klog, int v) {
-    static const strip_fn table[4][2] = {
-        {strip_kernel<R, 1, 1>, strip_kernel<R, 1, 2>},
-        {strip_kernel<R, 2, 1>, strip_kernel<R, 2, 2>},
-        {strip_kernel<R, 4, 1>, strip_kernel<R, 4, 2>},
-        {strip_kernel<R, 8, 1>, strip_kernel<R, 8, 2>},
+static const std::vector<strip_variant>& variants_for() {
+    static const std::vector<strip_variant> v = {
+        make_variant<R, 1, 2, 1>(),  make_variant<R, 1, 1, 1>(),  make_variant<R, 1, 4, 1>(),
+        make_variant<R, 2, 2, 2>(),  make_variant<R, 2, 2, 1>(),  make_variant<R, 2, 1, 2>(),
+        make_variant<R, 4, 2, 4>(),  make_variant<R, 4, 2, 2>(),  make_variant<R, 4, 1, 4>(),
+        make_variant<R, 4, 4, 2>(),  make_variant<R, 8, 2, 4>(),  make_variant<R, 8, 2, 2>(),
+        make_variant<R, 8, 1, 8>(),  make_variant<R, 8, 1, 4>(),  make_variant<R, 8, 4, 2>(),
+        make_variant<R, 16, 2, 2>(), make_variant<R, 16, 2, 4>(), make_variant<R, 16, 4, 2>(),
+        make_variant<R, 16, 1, 4>(),
     };
-    return table[klog][v - 1];
+    return v;
 }
 
-static int klog_of(int k) { return k == 1 ? 0 : k == 2 ? 1 : k == 4 ? 2 : k == 8 ? 3 : -1; }
-
-static strip_fn strip_kernel_for(int automaton, int k, int v) {
-    const int kl = klog_of(k);
-    if (kl < 0 || v < 1 || v > 2) return nullptr;
+const std::vector<strip_variant>& strip_variants(int automaton) {
+    static const std::vector<strip_variant> none;
     switch (automaton) {
-    case 0: return strip_for<game_of_life>(kl, v);
-    case 1: return strip_for<wire>(kl, v);
-    case 2: return strip_for<excitable>(kl, v);
-    default: return nullptr;
+    case 0: return variants_for<game_of_life>();
+    case 1: return variants_for<wire>();
+    case 2: return variants_for<excitable>();
+    default: return none;
     }
+}
+
+const strip_variant* find_variant(int automaton, int k, int v, int l) {
+    for (const strip_variant& sv : strip_variants(automaton))
+        if (sv.k == k && (v == 0 || sv.v == v) && (l == 0 || sv.l == l)) return &sv;
+    return nullptr;
 }
 
 int planes_of(int automaton) {
@@ -91,45 +105,48 @@ void strip_counts(const grid_geom& g, int v, int tile_rows, int* nsx, int* nsy) 
     *nsy = (g.h + tile_rows - 1) / tile_rows;
 }
 
-int resident_strip_warps(int automaton, int k, int v) {
-    static std::mutex mu;
-    static int cache[kNumAutomata][4][2] = {};
+static int sm_count() {
     static int sms = 0;
-    const int kl = klog_of(k);
-    if (kl < 0 || automaton < 0 || automaton >= kNumAutomata || v < 1 || v > 2) return 0;
-    std::lock_guard<std::mutex> lock(mu);
     if (!sms) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (sms <= 0) sms = 1;
     }
-    int& slot = cache[automaton][kl][v - 1];
-    if (!slot) {
-        int blocks = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, strip_kernel_for(automaton, k, v),
-                                                      kStripWarpsPerBlock * 32, 0);
-        slot = std::max(1, blocks) * kStripWarpsPerBlock * sms;
-    }
-    return slot;
+    return sms;
 }
 
-int auto_tile_rows(const grid_geom& g, int k, int v) {
-    const int resident = resident_strip_warps(g.automaton, k, v);
+int resident_strip_tasks(const strip_variant& sv) {
+    static std::mutex mu;
+    static std::map<const void*, int> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(sv.fn);
+    if (it != cache.end()) return it->second;
+    cudaFuncSetAttribute(sv.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, sv.smem_bytes);
+    int blocks = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, sv.fn, sv.threads, sv.smem_bytes);
+    const int n = std::max(1, blocks) * sm_count();
+    cache[sv.fn] = n;
+    return n;
+}
+
+int auto_tile_rows(const grid_geom& g, const strip_variant& sv) {
+    const int resident = resident_strip_tasks(sv);
     int nsx, nsy;
-    strip_counts(g, v, 1, &nsx, &nsy);
+    strip_counts(g, sv.v, 1, &nsx, &nsy);
     // One wave: as many row tasks per column as fit beside the other columns.
     const int per_column = std::max(1, resident / std::max(1, nsx));
     int rows = (g.h + per_column - 1) / per_column;
     // Keep the 2K halo rows of each task small against its own rows.
-    rows = std::max(rows, 8 * k);
+    rows = std::max(rows, 8 * sv.k);
     return std::min(rows, (int)g.h);
 }
 
 cudaError_t launch_strip_pass(const grid_geom& g, const uint32_t* in, uint32_t* out, const run_plan& plan,
                               cudaStream_t stream) {
-    strip_fn fn = strip_kernel_for(g.automaton, plan.k, plan.v);
-    if (!fn) return cudaErrorInvalidValue;
+    const strip_variant* sv = find_variant(g.automaton, plan.k, plan.v, plan.l);
+    if (!sv) return cudaErrorInvalidValue;
+    resident_strip_tasks(*sv);  // sets the kernel's shared-memory attribute once
     strip_launch a;
     a.in = in;
     a.out = out;
@@ -139,9 +156,8 @@ cudaError_t launch_strip_pass(const grid_geom& g, const uint32_t* in, uint32_t* 
     a.tile_rows = plan.tile_rows;
     strip_counts(g, plan.v, plan.tile_rows, &a.nsx, &a.nsy);
     const int64_t tasks = (int64_t)a.nsx * a.nsy;
-    const unsigned blocks = (unsigned)((tasks + kStripWarpsPerBlock - 1) / kStripWarpsPerBlock);
-    fn<<<blocks, kStripWarpsPerBlock * 32, 0, stream>>>(a);
-    return cudaGetLastError();
+    void* args[] = {&a};
+    return cudaLaunchKernel(sv->fn, dim3((unsigned)tasks), dim3(sv->threads), args, (size_t)sv->smem_bytes, stream);
 }
 
 // ---------------------------------------------------------------------------

@@ -1,0 +1,184 @@
+// cb2_pipe.cuh -- the strip wavefront split across the warps of a CTA.
+//
+// Keeping all K levels of the temporal wavefront in the registers of one warp
+// makes the register count -- and with it the number of resident warps --
+// grow with K.  pipe_run splits the K levels over the W = K / L warps of a
+// CTA: warp w owns levels [w*L, (w+1)*L) of the same strip and the CTA
+// advances in lock step, one row per step:
+//
+//   warp 0      takes the next input row from a shared-memory ring that
+//               cp.async keeps DEPTH rows ahead (global loads never block a
+//               register), pushes it through its L levels
+//   warp w > 0  takes the row warp w-1 produced in the previous step from a
+//               double-buffered shared-memory slot, pushes it through its L
+//               levels
+//   warp W-1    writes the finished row (generation t+K) to global memory
+//
+// One __syncthreads per step separates the slot a warp writes from the slot
+// its successor reads.  The row bookkeeping is the single-warp wavefront's:
+// input row r (sweep coordinates) leaves warp W-1 at step r + W - 1 as output
+// row r - K, so rows before the 2K-row warm-up are computed but never stored.
+#pragma once
+
+#include <cstdint>
+#include <type_traits>
+
+#include "cb2_strip.cuh"
+
+namespace cb2 {
+
+template <int V>
+struct pipe_vec;  // one lane's V words as a single shared-memory access
+template <>
+struct pipe_vec<1> {
+    using type = uint32_t;
+};
+template <>
+struct pipe_vec<2> {
+    using type = uint2;
+};
+template <>
+struct pipe_vec<4> {
+    using type = uint4;
+};
+
+// Shared memory of one CTA in 32-bit words.
+template <class R, int K, int V, int L, int DEPTH>
+constexpr int pipe_smem_words() {
+    return (DEPTH + 2 * (K / L - 1)) * R::P * 32 * V;
+}
+
+__device__ __forceinline__ void cp_async4(uint32_t* smem, const uint32_t* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// A row slot in shared memory: plane p, lane l, word i at ((p*32)+l)*V + i.
+template <class R, int V>
+__device__ __forceinline__ void slot_read(const uint32_t* slot, int lane, uint32_t (&row)[V][R::P]) {
+    using vec = typename pipe_vec<V>::type;
+#pragma unroll
+    for (int p = 0; p < R::P; ++p) {
+        const vec v = reinterpret_cast<const vec*>(slot)[p * 32 + lane];
+        const uint32_t* w = reinterpret_cast<const uint32_t*>(&v);
+#pragma unroll
+        for (int i = 0; i < V; ++i) row[i][p] = w[i];
+    }
+}
+
+template <class R, int V>
+__device__ __forceinline__ void slot_write(uint32_t* slot, int lane, const uint32_t (&row)[V][R::P]) {
+    using vec = typename pipe_vec<V>::type;
+#pragma unroll
+    for (int p = 0; p < R::P; ++p) {
+        vec v;
+        uint32_t* w = reinterpret_cast<uint32_t*>(&v);
+#pragma unroll
+        for (int i = 0; i < V; ++i) w[i] = row[i][p];
+        reinterpret_cast<vec*>(slot)[p * 32 + lane] = v;
+    }
+}
+
+// Runs one strip task on the whole CTA (W = K / L warps, all active).
+// `smem` holds pipe_smem_words<R, K, V, L, DEPTH>() words, 16-byte aligned.
+template <class R, int K, int V, int L, int DEPTH>
+__device__ __forceinline__ void pipe_run(const strip_task& t, uint32_t* smem) {
+    static_assert(K % L == 0, "levels per warp must divide K");
+    static_assert(DEPTH >= 2, "input ring of at least two rows");
+    constexpr int W = K / L;
+    constexpr int P = R::P;
+    constexpr int SLOT = P * 32 * V;  // words per row slot
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+
+    int64_t col[V];
+    bool keep[V];
+#pragma unroll
+    for (int i = 0; i < V; ++i) {
+        const int off = V * lane + i;
+        int c = (t.x0 - 1 + off) % t.wd;
+        if (c < 0) c += t.wd;
+        col[i] = c;
+        keep[i] = off >= 1 && off <= t.nx;
+    }
+
+    strip_state<R, L, V> s;
+#pragma unroll
+    for (int g = 0; g < L; ++g)
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int i = 0; i < V; ++i) {
+#pragma unroll
+                for (int k = 0; k < R::NH; ++k) s.h[g][q][i][k] = 0;
+#pragma unroll
+                for (int p = 0; p < P; ++p) s.c[g][q][i][p] = 0;
+            }
+
+    uint32_t* ring = smem;                  // DEPTH input rows (warp 0)
+    uint32_t* hand = smem + DEPTH * SLOT;   // 2 slots per warp boundary
+    const int total = t.ny + 2 * K;         // rows entering warp 0
+    const int steps = total + W - 1;
+
+    // Warp 0 keeps DEPTH-1 input rows in flight.
+    int lr = 0;
+    auto issue = [&](int r) {
+        if (r < total) {
+            const uint32_t* base = t.in + (int64_t)lr * t.wd;
+            uint32_t* dst = ring + (r % DEPTH) * SLOT;
+#pragma unroll
+            for (int p = 0; p < P; ++p)
+#pragma unroll
+                for (int i = 0; i < V; ++i) cp_async4(dst + (p * 32 + lane) * V + i, base + p * t.plane_words + col[i]);
+            lr = lr + 1 == t.h ? 0 : lr + 1;
+        }
+        cp_async_commit();  // empty groups keep the count uniform
+    };
+    if (warp == 0) {
+        lr = (t.y0 - K) % t.h;
+        if (lr < 0) lr += t.h;
+#pragma unroll
+        for (int r = 0; r < DEPTH - 1; ++r) issue(r);
+    } else {
+        // the first reads of every hand-off slot see zeros (warm-up rows)
+        for (int j = lane; j < 2 * SLOT; j += 32) hand[(warp - 1) * 2 * SLOT + j] = 0;
+    }
+    __syncthreads();
+
+    auto step = [&](int st, auto parity) {
+        constexpr int Q = decltype(parity)::value;
+        uint32_t row[V][P];
+        if (warp == 0) {
+            issue(st + DEPTH - 1);
+            cp_async_wait<DEPTH - 1>();
+            if (st < total) slot_read<R, V>(ring + (st % DEPTH) * SLOT, lane, row);
+            else
+#pragma unroll
+                for (int i = 0; i < V; ++i)
+#pragma unroll
+                    for (int p = 0; p < P; ++p) row[i][p] = 0;
+        } else {
+            slot_read<R, V>(hand + ((warp - 1) * 2 + (st & 1)) * SLOT, lane, row);
+        }
+        strip_push<R, L, V, Q>(s, row);
+        if (warp == W - 1) {
+            const int r0 = st - (W - 1);  // input row whose result leaves now
+            if (r0 >= 2 * K && r0 < total) strip_store<R, V>(t, col, keep, t.y0 + r0 - 2 * K, row);
+        } else {
+            slot_write<R, V>(hand + (warp * 2 + ((st + 1) & 1)) * SLOT, lane, row);
+        }
+        __syncthreads();
+    };
+    for (int st = 0; st < steps; st += 2) {
+        step(st, std::integral_constant<int, 0>{});
+        if (st + 1 < steps) step(st + 1, std::integral_constant<int, 1>{});
+    }
+    if (warp == 0) cp_async_wait<0>();
+}
+
+} // namespace cb2

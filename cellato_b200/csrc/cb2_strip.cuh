@@ -1,18 +1,18 @@
-// cb2_strip.cuh -- the hot path: K generations of a bit-plane strip per HBM
-// round trip, held entirely in registers.
+// cb2_strip.cuh -- the hot path's building blocks: a strip task and the
+// register wavefront that advances one strip row through L generations.
 //
-// Work unit ("strip task"): one warp owns a vertical strip of the grid.  Lane
-// l holds V consecutive 32-bit words of every row, so the warp covers 32*V
-// words: words 1 .. 32*V-2 of the segment are the strip's own columns and the
-// two end words are its x halo.  The warp sweeps the strip top to bottom,
-// reading each input row once (plus K halo rows above and below) and writing
-// each output row once.
+// Work unit ("strip task"): a vertical strip of the grid.  Lane l of a warp
+// holds V consecutive 32-bit words of every row, so a warp covers 32*V words:
+// words 1 .. 32*V-2 of the segment are the strip's own columns and the two
+// end words are its x halo.  The strip is swept top to bottom; each input row
+// is read once (plus K halo rows above and below) and each output row is
+// written once (cb2_pipe.cuh drives the sweep).
 //
-// Temporal blocking is a register wavefront: level g (0 <= g < K) keeps the
-// horizontal aggregates and centre states of its two most recent rows.  When
-// a row of level g arrives, the row above it advances to level g+1 and is
-// handed to level g+1 in the same pass, so one input row of generation t
-// turns into one output row of generation t+K, K rows further up.
+// Temporal blocking is a register wavefront: level g keeps the horizontal
+// aggregates and centre states of its two most recent rows.  When a row of
+// level g arrives, the row above it advances to level g+1 and is handed to
+// level g+1 in the same pass, so one row pushed through L levels leaves as
+// the row L rows further up, L generations later.
 //
 // Neighbours: left/right words come from the adjacent lanes through warp
 // shuffles, and cells x-1 / x+1 are formed with funnel shifts across word
@@ -88,16 +88,6 @@ __device__ __forceinline__ void strip_push(strip_state<R, K, V>& s, uint32_t (&r
 }
 
 template <class R, int V>
-__device__ __forceinline__ void strip_load(const strip_task& t, const int64_t (&col)[V], int row_idx,
-                                           uint32_t (&dst)[V][R::P]) {
-    const uint32_t* base = t.in + (int64_t)row_idx * t.wd;
-#pragma unroll
-    for (int p = 0; p < R::P; ++p)
-#pragma unroll
-        for (int i = 0; i < V; ++i) dst[i][p] = __ldg(base + p * t.plane_words + col[i]);
-}
-
-template <class R, int V>
 __device__ __forceinline__ void strip_store(const strip_task& t, const int64_t (&col)[V], const bool (&keep)[V],
                                             int row_idx, const uint32_t (&src)[V][R::P]) {
     uint32_t* base = t.out + (int64_t)row_idx * t.wd;
@@ -106,59 +96,6 @@ __device__ __forceinline__ void strip_store(const strip_task& t, const int64_t (
 #pragma unroll
         for (int i = 0; i < V; ++i)
             if (keep[i]) base[p * t.plane_words + col[i]] = src[i][p];
-}
-
-// Runs one strip task on the calling warp (all 32 lanes must be active).
-template <class R, int K, int V>
-__device__ __forceinline__ void strip_run(const strip_task& t) {
-    static_assert(K >= 1 && K <= 32, "halo words cover at most 32 generations");
-    constexpr int P = R::P;
-    const int lane = threadIdx.x & 31;
-
-    int64_t col[V];
-    bool keep[V];
-#pragma unroll
-    for (int i = 0; i < V; ++i) {
-        const int off = V * lane + i;  // segment word, 0 and 32V-1 are halo
-        int c = (t.x0 - 1 + off) % t.wd;
-        if (c < 0) c += t.wd;
-        col[i] = c;
-        keep[i] = off >= 1 && off <= t.nx;
-    }
-
-    strip_state<R, K, V> s;
-#pragma unroll
-    for (int g = 0; g < K; ++g)
-#pragma unroll
-        for (int q = 0; q < 2; ++q)
-#pragma unroll
-            for (int i = 0; i < V; ++i) {
-#pragma unroll
-                for (int k = 0; k < R::NH; ++k) s.h[g][q][i][k] = 0;
-#pragma unroll
-                for (int p = 0; p < P; ++p) s.c[g][q][i][p] = 0;
-            }
-
-    const int total = t.ny + 2 * K;  // input rows swept
-    int rr = (t.y0 - K) % t.h;        // physical row of the next input row
-    if (rr < 0) rr += t.h;
-    auto advance = [&](int r) { return r + 1 == t.h ? 0 : r + 1; };
-
-    uint32_t a[V][P], b[V][P];
-    strip_load<R, V>(t, col, rr, a);
-    for (int it = 0; it < total; it += 2) {
-        // even row: prefetch the odd row, then push the even row
-        rr = advance(rr);
-        if (it + 1 < total) strip_load<R, V>(t, col, rr, b);
-        strip_push<R, K, V, 0>(s, a);
-        if (it >= 2 * K) strip_store<R, V>(t, col, keep, t.y0 + it - 2 * K, a);
-        if (it + 1 >= total) break;
-        // odd row: prefetch the next even row, then push the odd row
-        rr = advance(rr);
-        if (it + 2 < total) strip_load<R, V>(t, col, rr, a);
-        strip_push<R, K, V, 1>(s, b);
-        if (it + 1 >= 2 * K) strip_store<R, V>(t, col, keep, t.y0 + it + 1 - 2 * K, b);
-    }
 }
 
 } // namespace cb2

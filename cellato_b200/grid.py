@@ -185,8 +185,8 @@ class DeviceGrid:
 
     # the hot path -----------------------------------------------------------------------------
     def run(self, steps: int, temporal_steps: int = 0, tile_rows: int = 0, words_per_lane: int = 0,
-            stream=None) -> None:
-        t = _abi.tuning(temporal_steps, tile_rows, words_per_lane)
+            levels_per_warp: int = 0, stream=None) -> None:
+        t = _abi.tuning(temporal_steps, tile_rows, words_per_lane, levels_per_warp)
         check(lib.cb2_grid_run(self._h, steps, ctypes.byref(t), _stream_handle(stream)), "run")
 
     def checksum(self, values=None, stream=None) -> list[int]:
@@ -214,20 +214,21 @@ class DeviceGrid:
 
 
 def plan(automaton, x_size: int, y_size: int, temporal_steps: int = 0, tile_rows: int = 0,
-         words_per_lane: int = 0) -> dict:
-    """The plan (temporal depth, strip height, lane width) a run would use."""
-    want = _abi.tuning(temporal_steps, tile_rows, words_per_lane)
+         words_per_lane: int = 0, levels_per_warp: int = 0) -> dict:
+    """The plan (temporal depth, strip height, lane width, levels per warp) a run would use."""
+    want = _abi.tuning(temporal_steps, tile_rows, words_per_lane, levels_per_warp)
     got = _abi.Tuning()
     check(lib.cb2_plan(automaton_id(automaton), x_size, y_size, ctypes.byref(want), ctypes.byref(got)), "plan")
     return got.as_dict()
 
 
 def run_bit_planes(automaton, a_planes: list[int], b_planes: list[int], x_size: int, y_size: int, steps: int,
-                   temporal_steps: int = 0, tile_rows: int = 0, words_per_lane: int = 0, stream=None) -> bool:
+                   temporal_steps: int = 0, tile_rows: int = 0, words_per_lane: int = 0, levels_per_warp: int = 0,
+                   stream=None) -> bool:
     """Advances caller-owned device planes; returns True if the result is in ``b_planes``."""
     a = (ctypes.c_void_p * len(a_planes))(*a_planes)
     b = (ctypes.c_void_p * len(b_planes))(*b_planes)
-    t = _abi.tuning(temporal_steps, tile_rows, words_per_lane)
+    t = _abi.tuning(temporal_steps, tile_rows, words_per_lane, levels_per_warp)
     res = ctypes.c_int()
     check(lib.cb2_run_bit_planes(automaton_id(automaton), a, b, x_size, y_size, steps, ctypes.byref(t),
                                  _stream_handle(stream), ctypes.byref(res)), "run_bit_planes")

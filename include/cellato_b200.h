@@ -75,9 +75,11 @@ int cb2_automaton_info(int id, const char** name, int* planes, int* states);
  * Replaces --temporal_steps / --temporal_tile_size_y / --cuda_block_size_*
  * (experiments/run_params.hpp:10-43). */
 typedef struct cb2_tuning {
-    int temporal_steps; /* generations per HBM round trip: 1, 2, 4 or 8     */
-    int tile_rows;      /* output rows per warp strip                       */
-    int words_per_lane; /* 32-bit words per lane: 1 or 2                    */
+    int temporal_steps;  /* generations per HBM round trip: 1, 2, 4, 8, 16  */
+    int tile_rows;       /* output rows per strip task (one CTA)            */
+    int words_per_lane;  /* 32-bit words per lane: 1, 2 or 4                */
+    int levels_per_warp; /* generations each warp of the CTA holds; the CTA
+                            has temporal_steps / levels_per_warp warps      */
 } cb2_tuning;
 
 /* ---- caller-owned device planes ----------------------------------------- */
@@ -138,7 +140,7 @@ int64_t cb2_grid_time_step(const cb2_grid* grid);
  * time spent (<= 0: a default). */
 int cb2_autotune(int automaton, int64_t x_size, int64_t y_size, double budget_ms, cb2_tuning* best);
 /* Loads / saves the tuning table as text lines
- * "automaton x_size y_size temporal_steps tile_rows words_per_lane". */
+ * "automaton x_size y_size temporal_steps tile_rows words_per_lane levels_per_warp". */
 int cb2_tuning_load(const char* path);
 int cb2_tuning_save(const char* path);
 /* The plan cb2_grid_run would use for a chunk of `steps` generations. */

@@ -60,13 +60,13 @@ def test_grid_create_rejects_bad_sizes_without_touching_the_gpu():
 
 def test_tuning_file_round_trip(tmp_path):
     p = tmp_path / "tune.txt"
-    p.write_text("# comment\ngame-of-life 65536 65536 8 950 2\nwire 32768 32768 4 512 2\n")
+    p.write_text("# comment\ngame-of-life 65536 65536 8 950 2 4\nwire 32768 32768 16 512 2 2\n")
     assert cb.tuning_load(str(p)) == 2
     out = tmp_path / "out.txt"
     assert cb.tuning_save(str(out)) >= 2
-    assert "game-of-life 65536 65536 8 950 2" in out.read_text()
+    assert "game-of-life 65536 65536 8 950 2 4" in out.read_text()
     bad = tmp_path / "bad.txt"
-    bad.write_text("game-of-life 64 64 3 10 2\n")
+    bad.write_text("game-of-life 64 64 3 10 2 1\n")
     with pytest.raises(ValueError, match="invalid tuning"):
         cb.tuning_load(str(bad))
 

@@ -15,7 +15,14 @@ pytestmark = pytest.mark.gpu
 PROBS = {0: [0.5, 0.5], 1: [0.6, 0.05, 0.05, 0.3], 2: [0.125] * 8}
 PLANS = [dict(), dict(temporal_steps=1), dict(temporal_steps=2, words_per_lane=1),
          dict(temporal_steps=4, tile_rows=5), dict(temporal_steps=8, words_per_lane=2, tile_rows=1),
-         dict(temporal_steps=8, words_per_lane=1, tile_rows=64)]
+         dict(temporal_steps=8, words_per_lane=1, tile_rows=64), dict(temporal_steps=8, words_per_lane=4),
+         dict(temporal_steps=16, words_per_lane=2, levels_per_warp=2),
+         dict(temporal_steps=16, words_per_lane=1, levels_per_warp=4, tile_rows=3),
+         dict(temporal_steps=8, words_per_lane=2, levels_per_warp=2)]
+# every instantiated (K, V, L)
+VARIANTS = [(1, 2, 1), (1, 1, 1), (1, 4, 1), (2, 2, 2), (2, 2, 1), (2, 1, 2), (4, 2, 4), (4, 2, 2), (4, 1, 4),
+            (4, 4, 2), (8, 2, 4), (8, 2, 2), (8, 1, 8), (8, 1, 4), (8, 4, 2), (16, 2, 2), (16, 2, 4), (16, 4, 2),
+            (16, 1, 4)]
 
 
 def device_run(automaton, cells, steps, **plan):
@@ -53,12 +60,13 @@ def test_golden_cases(cuda, golden, plan):
 
 def test_random_shapes_and_plans(cuda):
     rng = random.Random(2024)
-    for trial in range(60):
+    for trial in range(120):
         a = rng.randrange(3)
         x = 32 * rng.choice([1, 2, 3, 5, 29, 30, 31, 32, 61, 62, 63, 64, 65, 97])
         y = rng.choice([1, 2, 3, 7, 16, 17, 64, 101])
         steps = rng.randrange(0, 40)
-        plan = dict(temporal_steps=rng.choice([0, 1, 2, 4, 8]), words_per_lane=rng.choice([0, 1, 2]),
+        k, v, lv = rng.choice(VARIANTS)
+        plan = dict(temporal_steps=k, words_per_lane=v, levels_per_warp=lv,
                     tile_rows=rng.choice([0, 1, 2, 3, 9, 1000]))
         cells = O.init_cells(x, y, trial, O.thresholds(PROBS[a]))
         got, ck = device_run(a, cells, steps, **plan)
@@ -132,6 +140,28 @@ def test_invalid_state_is_rejected(cuda):
             g.upload_cells(cells)
 
 
+def test_every_variant_on_a_ragged_grid(cuda):
+    # 4 strips wide with a ragged last strip, ragged last row tile, wrap on both axes.
+    x, y, steps = 32 * 200, 37, 33
+    for a in (0, 1, 2):
+        cells = O.init_cells(x, y, 1234 + a, O.thresholds(PROBS[a]))
+        want = O.run_standard(a, cells, steps)
+        for (k, v, lv) in VARIANTS:
+            got, _ = device_run(a, cells, steps, temporal_steps=k, words_per_lane=v, levels_per_warp=lv,
+                                tile_rows=11)
+            assert (got == want).all(), (a, k, v, lv)
+
+
+def test_plan_resolution(cuda):
+    p = cb.plan("game-of-life", 65536, 65536, temporal_steps=8, words_per_lane=2, levels_per_warp=4)
+    assert (p["temporal_steps"], p["words_per_lane"], p["levels_per_warp"]) == (8, 2, 4)
+    assert p["tile_rows"] >= 64
+    with pytest.raises(ValueError, match="no strip kernel"):
+        cb.plan("game-of-life", 4096, 4096, temporal_steps=2, words_per_lane=4, levels_per_warp=2)
+    with pytest.raises(ValueError, match="temporal_steps must be"):
+        cb.plan("wire", 4096, 4096, temporal_steps=3)
+
+
 def test_caller_owned_planes(cuda):
     torch = cuda
     for a in (0, 1, 2):
@@ -169,8 +199,8 @@ def test_glider_crosses_the_torus(cuda):
     for n in (32, 64, 96):
         cells = np.zeros((n, n), dtype=np.uint8)
         for (yy, xx) in [(0, 1), (1, 2), (2, 0), (2, 1), (2, 2)]:
-            cells[yy + 5, xx + n - 2] = 1  # straddles the x wrap
-        for plan in (dict(temporal_steps=8), dict(temporal_steps=1, words_per_lane=1)):
+            cells[(yy + 5) % n, (xx + n - 2) % n] = 1  # straddles the x wrap
+        for plan in (dict(temporal_steps=8), dict(temporal_steps=1, words_per_lane=1), dict(temporal_steps=16)):
             got, _ = device_run(0, cells, 4 * n, **plan)
             assert (got == cells).all(), (n, plan)
             shifted, _ = device_run(0, cells, 4, **plan)
@@ -184,7 +214,8 @@ def test_full_size_plans_agree(cuda):
     thr = cb.thresholds([0.65, 0.35])
     first = None
     sums = []
-    for plan in (dict(temporal_steps=8), dict(temporal_steps=1), dict(temporal_steps=4, words_per_lane=1)):
+    for plan in (dict(temporal_steps=8), dict(temporal_steps=1), dict(temporal_steps=4, words_per_lane=1),
+                 dict(temporal_steps=16, words_per_lane=4)):
         with cb.DeviceGrid(0, x, y) as g:
             g.fill_random(99, thr=thr)
             g.run(16, **plan)
@@ -194,7 +225,7 @@ def test_full_size_plans_agree(cuda):
                 first = img
             else:
                 assert np.array_equal(img, first), plan
-    assert sums[0] == sums[1] == sums[2]
+    assert all(s == sums[0] for s in sums)
     assert sum(sums[0]) > 0
 
 
