@@ -96,7 +96,7 @@ static bool valid_k(int k) { return k == 1 || k == 2 || k == 4 || k == 8 || k ==
 
 // Default (K, V, L) per automaton, the fastest plans measured on B200 at the
 // headline sizes; cb2_autotune replaces them per size.
-static const int kDefaultPlan[kNumAutomata][3] = {{8, 2, 4}, {16, 2, 2}, {8, 1, 8}};
+static const int kDefaultPlan[kNumAutomata][3] = {{8, 1, 8}, {16, 2, 2}, {16, 1, 16}};
 
 // Fills every 0 field of `t` for a grid of geometry g.
 static int resolve_plan(const grid_geom& g, const cb2_tuning* t, run_plan* plan) {

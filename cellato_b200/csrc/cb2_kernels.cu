@@ -49,13 +49,16 @@ __global__ void __launch_bounds__(32 * (K / L)) pipe_kernel(strip_launch a) {
     t.nx = min(own, a.wd - t.x0);
     t.y0 = sy * a.tile_rows;
     t.ny = min(a.tile_rows, a.h - t.y0);
-    pipe_run<R, K, V, L, kRingDepth>(t, smem);
+    if constexpr (L == K)
+        warp_run<R, K, V, kRingDepth>(t, smem);  // one warp, skewed levels
+    else
+        pipe_run<R, K, V, L, kRingDepth>(t, smem);
 }
 
 template <class R, int K, int V, int L>
 static strip_variant make_variant() {
-    return strip_variant{K, V, L, (const void*)pipe_kernel<R, K, V, L>, 32 * (K / L),
-                         4 * pipe_smem_words<R, K, V, L, kRingDepth>()};
+    const int words = L == K ? warp_smem_words<R, V, kRingDepth>() : pipe_smem_words<R, K, V, L, kRingDepth>();
+    return strip_variant{K, V, L, (const void*)pipe_kernel<R, K, V, L>, 32 * (K / L), 4 * words};
 }
 
 // The instantiated (K, V, L) plans; for each (K, V) the first entry is the
@@ -69,7 +72,8 @@ static const std::vector<strip_variant>& variants_for() {
         make_variant<R, 4, 4, 2>(),  make_variant<R, 8, 2, 4>(),  make_variant<R, 8, 2, 2>(),
         make_variant<R, 8, 1, 8>(),  make_variant<R, 8, 1, 4>(),  make_variant<R, 8, 4, 2>(),
         make_variant<R, 16, 2, 2>(), make_variant<R, 16, 2, 4>(), make_variant<R, 16, 4, 2>(),
-        make_variant<R, 16, 1, 4>(),
+        make_variant<R, 16, 1, 4>(), make_variant<R, 8, 2, 8>(),  make_variant<R, 16, 1, 16>(),
+        make_variant<R, 4, 4, 4>(),
     };
     return v;
 }

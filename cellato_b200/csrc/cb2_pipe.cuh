@@ -181,4 +181,86 @@ __device__ __forceinline__ void pipe_run(const strip_task& t, uint32_t* smem) {
     if (warp == 0) cp_async_wait<0>();
 }
 
+// Shared memory of one warp-strip (skewed single-warp kernel) in 32-bit words.
+template <class R, int V, int DEPTH>
+constexpr int warp_smem_words() {
+    return DEPTH * R::P * 32 * V;
+}
+
+// Runs one strip task on one warp with all K levels in registers, in the
+// skewed order of skewed_step: every level of a step is independent, so a
+// warp has K*V independent chains to issue from.  Input rows stream through
+// a cp.async ring of DEPTH rows in `smem` (warp_smem_words words); there is
+// no barrier.  A row entering at step s leaves level K-1 at step s+K-1 as
+// the row K rows above it: output sweep row s - 2K + 1.
+template <class R, int K, int V, int DEPTH>
+__device__ __forceinline__ void warp_run(const strip_task& t, uint32_t* smem) {
+    constexpr int P = R::P;
+    constexpr int SLOT = P * 32 * V;
+    const int lane = threadIdx.x & 31;
+
+    int64_t col[V];
+    bool keep[V];
+#pragma unroll
+    for (int i = 0; i < V; ++i) {
+        const int off = V * lane + i;
+        int c = (t.x0 - 1 + off) % t.wd;
+        if (c < 0) c += t.wd;
+        col[i] = c;
+        keep[i] = off >= 1 && off <= t.nx;
+    }
+
+    strip_state<R, K, V> s;
+    uint32_t pend[K][V][P];
+#pragma unroll
+    for (int g = 0; g < K; ++g)
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+#pragma unroll
+                for (int k = 0; k < R::NH; ++k) s.h[g][q][i][k] = 0;
+#pragma unroll
+                for (int p = 0; p < P; ++p) s.c[g][q][i][p] = 0;
+            }
+#pragma unroll
+            for (int p = 0; p < P; ++p) pend[g][i][p] = 0;
+        }
+
+    const int total = t.ny + 2 * K;  // input rows
+    const int steps = total + K - 1;
+    int lr = (t.y0 - K) % t.h;
+    if (lr < 0) lr += t.h;
+    auto issue = [&](int r) {
+        if (r < total) {
+            const uint32_t* base = t.in + (int64_t)lr * t.wd;
+            uint32_t* dst = smem + (r % DEPTH) * SLOT;
+#pragma unroll
+            for (int p = 0; p < P; ++p)
+#pragma unroll
+                for (int i = 0; i < V; ++i) cp_async4(dst + (p * 32 + lane) * V + i, base + p * t.plane_words + col[i]);
+            lr = lr + 1 == t.h ? 0 : lr + 1;
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int r = 0; r < DEPTH - 1; ++r) issue(r);
+
+    auto step = [&](int st, auto parity) {
+        constexpr int S = decltype(parity)::value;
+        issue(st + DEPTH - 1);
+        cp_async_wait<DEPTH - 1>();
+        if (st < total) slot_read<R, V>(smem + (st % DEPTH) * SLOT, lane, pend[0]);
+        uint32_t out[V][P];
+        skewed_step<R, K, V, S>(s, pend, out);
+        const int j = st - 2 * K + 1;  // output sweep row
+        if (j >= K && j < K + t.ny) strip_store<R, V>(t, col, keep, t.y0 + j - K, out);
+    };
+    for (int st = 0; st < steps; st += 2) {
+        step(st, std::integral_constant<int, 0>{});
+        if (st + 1 < steps) step(st + 1, std::integral_constant<int, 1>{});
+    }
+    cp_async_wait<0>();
+}
+
 } // namespace cb2

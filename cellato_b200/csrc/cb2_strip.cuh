@@ -87,6 +87,64 @@ __device__ __forceinline__ void strip_push(strip_state<R, K, V>& s, uint32_t (&r
     }
 }
 
+// One wavefront level: pushes `row` (a row of level g, parity slot Q) into
+// the level's window and returns, in `row`, the row above it advanced one
+// generation.
+template <class R, int K, int V, int Q>
+__device__ __forceinline__ void level_push(strip_state<R, K, V>& s, int g, uint32_t (&row)[V][R::P]) {
+    constexpr int P = R::P, NH = R::NH;
+    uint32_t ind[V];
+#pragma unroll
+    for (int i = 0; i < V; ++i) ind[i] = R::indicator(row[i]);
+    const uint32_t lw = __shfl_up_sync(kFullMask, ind[V - 1], 1);
+    const uint32_t rw = __shfl_down_sync(kFullMask, ind[0], 1);
+    uint32_t hc[V][NH];
+#pragma unroll
+    for (int i = 0; i < V; ++i) {
+        const uint32_t l = i == 0 ? lw : ind[i - 1];
+        const uint32_t r = i == V - 1 ? rw : ind[i + 1];
+        R::hagg(west_of(l, ind[i]), ind[i], east_of(ind[i], r), hc[i]);
+    }
+    uint32_t nxt[V][P];
+#pragma unroll
+    for (int i = 0; i < V; ++i) R::next(s.h[g][Q][i], s.h[g][1 - Q][i], hc[i], s.c[g][1 - Q][i], nxt[i]);
+#pragma unroll
+    for (int i = 0; i < V; ++i) {
+#pragma unroll
+        for (int k = 0; k < NH; ++k) s.h[g][Q][i][k] = hc[i][k];
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            s.c[g][Q][i][p] = row[i][p];
+            row[i][p] = nxt[i][p];
+        }
+    }
+}
+
+// Skewed wavefront step: level g takes the row level g-1 produced in the
+// previous step (held in pend[g]), so the K levels of one step are
+// independent of each other.  pend[0] is the new input row; on return
+// `out` holds the row leaving level K-1 and pend[g] the input of level g for
+// the next step.  Level g receives row s - 2g at step s, so every level's
+// rows alternate parity with the step parity S.
+template <class R, int K, int V, int S>
+__device__ __forceinline__ void skewed_step(strip_state<R, K, V>& s, uint32_t (&pend)[K][V][R::P],
+                                            uint32_t (&out)[V][R::P]) {
+#pragma unroll
+    for (int g = 0; g < K; ++g) {
+        level_push<R, K, V, S>(s, g, pend[g]);
+    }
+#pragma unroll
+    for (int i = 0; i < V; ++i)
+#pragma unroll
+        for (int p = 0; p < R::P; ++p) out[i][p] = pend[K - 1][i][p];
+#pragma unroll
+    for (int g = K - 1; g > 0; --g)
+#pragma unroll
+        for (int i = 0; i < V; ++i)
+#pragma unroll
+            for (int p = 0; p < R::P; ++p) pend[g][i][p] = pend[g - 1][i][p];
+}
+
 template <class R, int V>
 __device__ __forceinline__ void strip_store(const strip_task& t, const int64_t (&col)[V], const bool (&keep)[V],
                                             int row_idx, const uint32_t (&src)[V][R::P]) {

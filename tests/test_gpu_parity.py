@@ -22,7 +22,7 @@ PLANS = [dict(), dict(temporal_steps=1), dict(temporal_steps=2, words_per_lane=1
 # every instantiated (K, V, L)
 VARIANTS = [(1, 2, 1), (1, 1, 1), (1, 4, 1), (2, 2, 2), (2, 2, 1), (2, 1, 2), (4, 2, 4), (4, 2, 2), (4, 1, 4),
             (4, 4, 2), (8, 2, 4), (8, 2, 2), (8, 1, 8), (8, 1, 4), (8, 4, 2), (16, 2, 2), (16, 2, 4), (16, 4, 2),
-            (16, 1, 4)]
+            (16, 1, 4), (8, 2, 8), (16, 1, 16), (4, 4, 4)]
 
 
 def device_run(automaton, cells, steps, **plan):
