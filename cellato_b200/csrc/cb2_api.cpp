@@ -130,7 +130,7 @@ static int resolve_plan(const grid_geom& g, const cb2_tuning* t, run_plan* plan)
     return CB2_OK;
 }
 
-static int make_geom(int automaton, int64_t x, int64_t y, grid_geom* g) {
+int make_geom(int automaton, int64_t x, int64_t y, grid_geom* g) {
     const int P = planes_of(automaton);
     if (P < 0) return fail(CB2_ENOTFOUND, "unknown automaton id " + std::to_string(automaton));
     if (x <= 0 || y <= 0) return fail(CB2_EINVAL, "grid sizes must be positive");
@@ -148,8 +148,8 @@ static int make_geom(int automaton, int64_t x, int64_t y, grid_geom* g) {
 
 // Launches `steps` generations from `cur` (buffer index) alternating with
 // the other buffer; returns the index that holds the result.
-static int run_chunks(const grid_geom& g, uint32_t* const bufs[2], int cur, int64_t steps, const cb2_tuning* tuning,
-                      cudaStream_t stream, int* result) {
+int run_chunks(const grid_geom& g, uint32_t* const bufs[2], int cur, int64_t steps, const cb2_tuning* tuning,
+               cudaStream_t stream, int* result) {
     run_plan main_plan;
     int rc = resolve_plan(g, tuning, &main_plan);
     if (rc) return rc;

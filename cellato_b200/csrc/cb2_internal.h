@@ -85,4 +85,17 @@ constexpr int kLop3ProbeOpsPerIter = 64;
 // Thread-local error message for cb2_last_error().
 void set_error(const std::string& msg);
 
+}  // namespace cb2
+
+struct cb2_tuning;
+
+namespace cb2 {
+
+// Validates a grid size for an automaton and fills its geometry.
+int make_geom(int automaton, int64_t x, int64_t y, grid_geom* g);
+// Launches `steps` generations starting in bufs[cur], alternating between the
+// two buffers; *result is the index of the buffer holding the result.
+int run_chunks(const grid_geom& g, uint32_t* const bufs[2], int cur, int64_t steps, const cb2_tuning* tuning,
+               cudaStream_t stream, int* result);
+
 } // namespace cb2

@@ -93,6 +93,26 @@ typedef struct cb2_tuning {
 int cb2_run_bit_planes(int automaton, void* const* a, void* const* b, int64_t x_size, int64_t y_size, int64_t steps,
                        const cb2_tuning* tuning, void* stream, int* result_in_b);
 
+/* Bytes of the static device scratch behind cb2_run_bit_planes_in_place. */
+#define CB2_STATIC_SCRATCH_BYTES (16u << 20)
+
+/* Allocation-free form of cb2_run_bit_planes for callers that cannot call
+ * cudaMalloc (a host application that owns all device memory and forbids
+ * plugins to allocate, or a step loop that must not allocate).  It has no
+ * counterpart in the reference.  `planes` (P consecutive planes in one
+ * allocation, CB2_LAYOUT_BIT_PLANES) hold the input and, in stream order,
+ * receive generation `steps`.  The second buffer of the double buffer is a
+ * file-scope __device__ array of CB2_STATIC_SCRATCH_BYTES that every GPU
+ * loading this library holds until exit; grids whose planes are larger are
+ * rejected with CB2_EINVAL.  No cudaMalloc / cudaFree or allocating routine
+ * is called.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  All calls on a device share the array, so
+ * calls that overlap on the GPU (different streams, or different host
+ * threads) race; serialise them. */
+int cb2_run_bit_planes_in_place(int automaton, void* const* planes, int64_t x_size, int64_t y_size, int64_t steps,
+                                const cb2_tuning* tuning, void* stream);
+
 /* ---- owning device grids -------------------------------------------------- */
 /* A device-resident grid: P bit-planes, double-buffered, generation counter.
  * Mirrors grid::to_cuda / to_cpu / free_cuda_memory of the reference layouts
