@@ -182,6 +182,129 @@ def traffic_for(kernel_key: str):
         return None
 
 
+BATCH_PROBS = {0: [0.65, 0.35], 1: [0.60, 0.05, 0.05, 0.30], 2: [0.125] * 8}
+
+
+def batch_workload(n: int, seed: int = 2024):
+    """4096 independent grids: sides log-uniform in [64, 4096] (widths rounded to
+    multiples of 32), automaton uniform over the three, steps log-uniform in
+    [10, 1000]."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    lo, hi = math.log(64), math.log(4096)
+    specs = []
+    for i in range(n):
+        x = int(min(4096, max(64, 32 * round(math.exp(rng.uniform(lo, hi)) / 32))))
+        y = int(min(4096, max(64, round(math.exp(rng.uniform(lo, hi))))))
+        a = int(rng.integers(0, 3))
+        steps = int(round(math.exp(rng.uniform(math.log(10), math.log(1000)))))
+        specs.append((a, x, y, steps))
+    return specs
+
+
+def bench_batch(cb, torch, stream, n: int, runs: int) -> dict:
+    specs = batch_workload(n)
+    grids = []
+    for i, (a, x, y, _) in enumerate(specs):
+        g = cb.DeviceGrid(a, x, y)
+        g.fill_random(1000 + i, BATCH_PROBS[a], stream=stream)
+        grids.append(g)
+    steps = [s for (_, _, _, s) in specs]
+    batch = cb.Batch(grids, steps)
+    info = batch.info()
+    for _ in range(2):
+        batch.run(stream)
+    batch.wait(stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(runs):
+        batch.run(stream)
+    e1.record(stream)
+    batch.wait(stream)
+    ms = e0.elapsed_time(e1) / runs
+    batch.run_per_grid(stream)  # warm-up of the per-grid plans
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    batch.run_per_grid(stream)
+    f1.record(stream)
+    f1.synchronize()
+    per_ms = f0.elapsed_time(f1)
+    batch.close()
+    for g in grids:
+        g.close()
+    cells = info["cell_updates"]
+    return {"workload": f"{n} grids, sides log-uniform [64,4096] (widths multiple of 32), automaton uniform "
+                        "{game-of-life, wire, excitable}, steps log-uniform [10,1000], seeded inits",
+            "value": cells / (ms * 1e-3) / 1e9, "unit": METRIC, "ms_per_run": ms, "runs": runs,
+            "cell_updates_per_run": cells, "tasks": info["tasks"], "persistent_ctas": info["persistent_ctas"],
+            "per_grid_value": cells / (per_ms * 1e-3) / 1e9, "per_grid_ms_per_run": per_ms,
+            "speedup_vs_per_grid": per_ms / ms,
+            "path": "cb2_batch_run (persistent tile-queue kernel, CUDA graph replay) vs cb2_batch_run_per_grid "
+                    "(cb2_grid_run per grid)"}
+
+
+def serve_workload(n: int, seed: int = 7):
+    """Requests: sides log-uniform in [128, 16384] (widths multiples of 32),
+    steps log-uniform in [1, 10000], automaton uniform, seeded inputs."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    lo, hi = math.log(128), math.log(16384)
+    out = []
+    for i in range(n):
+        x = int(min(16384, max(128, 32 * round(math.exp(rng.uniform(lo, hi)) / 32))))
+        y = int(min(16384, max(128, round(math.exp(rng.uniform(lo, hi))))))
+        steps = int(max(1, round(math.exp(rng.uniform(0.0, math.log(10000))))))
+        out.append((int(rng.integers(0, 3)), x, y, steps, 5000 + i))
+    return out
+
+
+def serve_stream(cb, specs, rate: float, per_request: bool, seed: int = 11) -> dict:
+    """Submits `specs` with Poisson arrivals at `rate` req/s; returns latency
+    percentiles (submit to result) and throughput over the makespan."""
+    import numpy as np
+
+    gaps = np.random.default_rng(seed).exponential(1.0 / rate, len(specs))
+    with cb.Server(per_request=per_request) as srv:
+        t0 = time.perf_counter()
+        due = 0.0
+        ids = []
+        for (a, x, y, steps, sd), gap in zip(specs, gaps):
+            due += gap
+            while time.perf_counter() - t0 < due:
+                time.sleep(min(0.0005, max(0.0, due - (time.perf_counter() - t0))))
+            ids.append(srv.submit(a, x, y, steps, sd, BATCH_PROBS[a]))
+        srv.drain(1200)
+        st = [srv.status(i) for i in ids]
+    lat = np.array([r["done_s"] - r["submit_s"] for r in st])
+    span = max(r["done_s"] for r in st) - min(r["submit_s"] for r in st)
+    cells = sum(x * y * steps for (_, x, y, steps, _) in specs)
+    return {"rate_req_s": rate, "requests": len(specs), "failed": sum(r["state"] != "done" for r in st),
+            "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "throughput": cells / span / 1e9, "makespan_s": span}
+
+
+def bench_serve(cb, n: int, rates) -> dict:
+    specs = serve_workload(n)
+    serve_stream(cb, specs[:20], 1000.0, False)  # warm-up: graph capture, pools
+    serve_stream(cb, specs[:20], 1000.0, True)
+    points = []
+    for rate in rates:
+        batched = serve_stream(cb, specs, rate, False)
+        plain = serve_stream(cb, specs, rate, True)
+        points.append({"rate_req_s": rate, "batched": batched, "per_request": plain,
+                       "throughput_ratio": batched["throughput"] / plain["throughput"]})
+    return {"workload": f"{n} requests per rate, Poisson arrivals, sides log-uniform [128,16384] (widths multiple "
+                        "of 32), steps log-uniform [1,10000], automaton uniform, seeded inits",
+            "unit": METRIC, "latency": "submit to finished (checksum ready), ms",
+            "memory_budget": "min(150 GiB, 80% of free device memory) of bit-plane state",
+            "path": "cb2_server (continuous batching, persistent batch kernel per round) vs cb2_server per_request=1 "
+                    "(one request at a time, one launch sequence each)",
+            "points": points}
+
+
 def launches_per_run(gens: int, k: int) -> int:
     n, left = 0, gens
     while left > 0:
@@ -202,6 +325,10 @@ def main() -> None:
     ap.add_argument("--workload", default="gol-65536", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=300)
+    ap.add_argument("--batch-grids", type=int, default=4096)
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
@@ -323,6 +450,15 @@ def main() -> None:
     e2e_wall = max_over_ranks(wall)
     e2e_value = world * cells * gens * args.steps / (e2e_ms * 1e-3) / 1e9
 
+    batched = None
+    if not args.no_batch:
+        grid.close()
+        batched = bench_batch(cb, torch, stream, args.batch_grids, max(3, args.steps))
+        grid = cb.DeviceGrid(a, x, y)
+    served = None
+    if not args.no_serve:
+        served = bench_serve(cb, args.serve_requests, [100.0, 1000.0, 5000.0, 20000.0])
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_sample(a, wl["probs"], args.cpu_seconds)
@@ -348,6 +484,8 @@ def main() -> None:
         "gpu_launches": launches,
         "clocks": clocks,
         "cpu_baseline": cpu,
+        "batched": batched,
+        "served": served,
     }
     print(json.dumps(out), flush=True)
 

@@ -57,6 +57,39 @@ class Tuning(ctypes.Structure):
                 "words_per_lane": self.words_per_lane, "levels_per_warp": self.levels_per_warp}
 
 
+class BatchOpts(ctypes.Structure):
+    _fields_ = [("temporal_steps", ctypes.c_int), ("tile_rows", ctypes.c_int), ("spin_limit", ctypes.c_longlong),
+                ("stall_task", ctypes.c_int)]
+
+
+class ServerOpts(ctypes.Structure):
+    _fields_ = [("memory_budget", ctypes.c_size_t), ("max_active", ctypes.c_int), ("chunk_steps", ctypes.c_int),
+                ("temporal_steps", ctypes.c_int), ("tile_rows", ctypes.c_int), ("per_request", ctypes.c_int),
+                ("task_capacity", ctypes.c_int), ("spin_limit", ctypes.c_longlong),
+                ("fail_alloc_at", ctypes.c_longlong), ("round_cells", ctypes.c_double)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("automaton", ctypes.c_int), ("x_size", ctypes.c_int64), ("y_size", ctypes.c_int64),
+                ("steps", ctypes.c_int64), ("seed", ctypes.c_uint64), ("n_thresholds", ctypes.c_int),
+                ("thresholds", ctypes.c_uint64 * 7), ("host_cells", ctypes.c_void_p),
+                ("host_result", ctypes.c_void_p)]
+
+
+class RequestStatus(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int), ("error", ctypes.c_int), ("steps_done", ctypes.c_int64),
+                ("submit_s", ctypes.c_double), ("admit_s", ctypes.c_double), ("done_s", ctypes.c_double),
+                ("checksum", ctypes.c_uint64 * 16)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
+                ("rounds", ctypes.c_int64), ("cell_updates", ctypes.c_double), ("used_bytes", ctypes.c_int64),
+                ("budget_bytes", ctypes.c_int64), ("now_s", ctypes.c_double)]
+
+
+REQ_QUEUED, REQ_ACTIVE, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
+
 _i64 = ctypes.c_int64
 _vp = ctypes.c_void_p
 _vpp = ctypes.POINTER(ctypes.c_void_p)
@@ -84,6 +117,19 @@ _SIGNATURES = {
     "cb2_grid_checksum": (ctypes.c_int, [_vp, _i64p, ctypes.c_int, _u64p, _vp]),
     "cb2_grid_planes": (ctypes.c_int, [_vp, _vpp, ctypes.POINTER(ctypes.c_int), _i64p]),
     "cb2_grid_time_step": (_i64, [_vp]),
+    "cb2_batch_create": (ctypes.c_int, [_vpp, _i64p, ctypes.c_int, ctypes.POINTER(BatchOpts), ctypes.POINTER(_vp)]),
+    "cb2_batch_destroy": (ctypes.c_int, [_vp]),
+    "cb2_batch_run": (ctypes.c_int, [_vp, _vp]),
+    "cb2_batch_wait": (ctypes.c_int, [_vp, _vp]),
+    "cb2_batch_run_per_grid": (ctypes.c_int, [_vp, _vp]),
+    "cb2_batch_info": (ctypes.c_int, [_vp, _i64p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]),
+    "cb2_server_create": (ctypes.c_int, [ctypes.POINTER(ServerOpts), ctypes.POINTER(_vp)]),
+    "cb2_server_submit": (ctypes.c_int, [_vp, ctypes.POINTER(Request), _i64p]),
+    "cb2_server_status": (ctypes.c_int, [_vp, _i64, ctypes.POINTER(RequestStatus)]),
+    "cb2_server_wait": (ctypes.c_int, [_vp, _i64, ctypes.c_double]),
+    "cb2_server_drain": (ctypes.c_int, [_vp, ctypes.c_double]),
+    "cb2_server_get_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ServerStats)]),
+    "cb2_server_destroy": (ctypes.c_int, [_vp]),
     "cb2_autotune": (ctypes.c_int, [ctypes.c_int, _i64, _i64, ctypes.c_double, _tp]),
     "cb2_tuning_load": (ctypes.c_int, [ctypes.c_char_p]),
     "cb2_tuning_save": (ctypes.c_int, [ctypes.c_char_p]),

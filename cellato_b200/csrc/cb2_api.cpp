@@ -177,17 +177,6 @@ int run_chunks(const grid_geom& g, uint32_t* const bufs[2], int cur, int64_t ste
 
 using namespace cb2;
 
-struct cb2_grid {
-    grid_geom g{};
-    uint32_t* buf[2] = {nullptr, nullptr};
-    int cur = 0;
-    int64_t time_step = 0;
-    void* staging = nullptr;  // device copy of a host image for layout conversion
-    size_t staging_bytes = 0;
-    unsigned* flag = nullptr;  // device error flag of the conversion kernels
-    unsigned long long* sums = nullptr;
-    int device = 0;
-};
 
 extern "C" {
 

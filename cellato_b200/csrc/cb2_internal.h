@@ -99,3 +99,16 @@ int run_chunks(const grid_geom& g, uint32_t* const bufs[2], int cur, int64_t ste
                cudaStream_t stream, int* result);
 
 } // namespace cb2
+
+// An owning device grid (the opaque cb2_grid of the C-ABI).
+struct cb2_grid {
+    cb2::grid_geom g{};
+    uint32_t* buf[2] = {nullptr, nullptr};  // the double buffer; buf[cur] holds the current generation
+    int cur = 0;
+    int64_t time_step = 0;
+    void* staging = nullptr;  // device copy of a host image for layout conversion
+    size_t staging_bytes = 0;
+    unsigned* flag = nullptr;  // device error flag of the conversion kernels
+    unsigned long long* sums = nullptr;
+    int device = 0;
+};

@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(32 * (K / L)) pipe_kernel(strip_launch a) {
     t.y0 = sy * a.tile_rows;
     t.ny = min(a.tile_rows, a.h - t.y0);
     if constexpr (L == K)
-        warp_run<R, K, V, kRingDepth>(t, smem);  // one warp, skewed levels
+        warp_run<R, K, V, kRingDepth>(t, strip_geom<V>(t, threadIdx.x & 31), smem);  // one warp, skewed levels
     else
         pipe_run<R, K, V, L, kRingDepth>(t, smem);
 }

@@ -95,17 +95,7 @@ __device__ __forceinline__ void pipe_run(const strip_task& t, uint32_t* smem) {
     constexpr int SLOT = P * 32 * V;  // words per row slot
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-
-    int64_t col[V];
-    bool keep[V];
-#pragma unroll
-    for (int i = 0; i < V; ++i) {
-        const int off = V * lane + i;
-        int c = (t.x0 - 1 + off) % t.wd;
-        if (c < 0) c += t.wd;
-        col[i] = c;
-        keep[i] = off >= 1 && off <= t.nx;
-    }
+    const lane_geom<V> geom = strip_geom<V>(t, lane);
 
     strip_state<R, L, V> s;
 #pragma unroll
@@ -134,7 +124,8 @@ __device__ __forceinline__ void pipe_run(const strip_task& t, uint32_t* smem) {
 #pragma unroll
             for (int p = 0; p < P; ++p)
 #pragma unroll
-                for (int i = 0; i < V; ++i) cp_async4(dst + (p * 32 + lane) * V + i, base + p * t.plane_words + col[i]);
+                for (int i = 0; i < V; ++i)
+                    cp_async4(dst + (p * 32 + lane) * V + i, base + p * t.plane_words + geom.col[i]);
             lr = lr + 1 == t.h ? 0 : lr + 1;
         }
         cp_async_commit();  // empty groups keep the count uniform
@@ -165,10 +156,10 @@ __device__ __forceinline__ void pipe_run(const strip_task& t, uint32_t* smem) {
         } else {
             slot_read<R, V>(hand + ((warp - 1) * 2 + (st & 1)) * SLOT, lane, row);
         }
-        strip_push<R, L, V, Q>(s, row);
+        strip_push<R, L, V, Q>(s, row, geom.src_l, geom.src_r);
         if (warp == W - 1) {
             const int r0 = st - (W - 1);  // input row whose result leaves now
-            if (r0 >= 2 * K && r0 < total) strip_store<R, V>(t, col, keep, t.y0 + r0 - 2 * K, row);
+            if (r0 >= 2 * K && r0 < total) strip_store<R, V>(t, geom, r0 - 2 * K, row);
         } else {
             slot_write<R, V>(hand + (warp * 2 + ((st + 1) & 1)) * SLOT, lane, row);
         }
@@ -194,21 +185,10 @@ constexpr int warp_smem_words() {
 // no barrier.  A row entering at step s leaves level K-1 at step s+K-1 as
 // the row K rows above it: output sweep row s - 2K + 1.
 template <class R, int K, int V, int DEPTH>
-__device__ __forceinline__ void warp_run(const strip_task& t, uint32_t* smem) {
+__device__ __forceinline__ void warp_run(const strip_task& t, const lane_geom<V>& geom, uint32_t* smem) {
     constexpr int P = R::P;
     constexpr int SLOT = P * 32 * V;
     const int lane = threadIdx.x & 31;
-
-    int64_t col[V];
-    bool keep[V];
-#pragma unroll
-    for (int i = 0; i < V; ++i) {
-        const int off = V * lane + i;
-        int c = (t.x0 - 1 + off) % t.wd;
-        if (c < 0) c += t.wd;
-        col[i] = c;
-        keep[i] = off >= 1 && off <= t.nx;
-    }
 
     strip_state<R, K, V> s;
     uint32_t pend[K][V][P];
@@ -229,7 +209,7 @@ __device__ __forceinline__ void warp_run(const strip_task& t, uint32_t* smem) {
 
     const int total = t.ny + 2 * K;  // input rows
     const int steps = total + K - 1;
-    int lr = (t.y0 - K) % t.h;
+    int lr = (t.y0 + geom.yoff - K) % t.h;  // this lane's next input row
     if (lr < 0) lr += t.h;
     auto issue = [&](int r) {
         if (r < total) {
@@ -238,7 +218,8 @@ __device__ __forceinline__ void warp_run(const strip_task& t, uint32_t* smem) {
 #pragma unroll
             for (int p = 0; p < P; ++p)
 #pragma unroll
-                for (int i = 0; i < V; ++i) cp_async4(dst + (p * 32 + lane) * V + i, base + p * t.plane_words + col[i]);
+                for (int i = 0; i < V; ++i)
+                    cp_async4(dst + (p * 32 + lane) * V + i, base + p * t.plane_words + geom.col[i]);
             lr = lr + 1 == t.h ? 0 : lr + 1;
         }
         cp_async_commit();
@@ -252,9 +233,9 @@ __device__ __forceinline__ void warp_run(const strip_task& t, uint32_t* smem) {
         cp_async_wait<DEPTH - 1>();
         if (st < total) slot_read<R, V>(smem + (st % DEPTH) * SLOT, lane, pend[0]);
         uint32_t out[V][P];
-        skewed_step<R, K, V, S>(s, pend, out);
+        skewed_step<R, K, V, S>(s, pend, out, geom.src_l, geom.src_r);
         const int j = st - 2 * K + 1;  // output sweep row
-        if (j >= K && j < K + t.ny) strip_store<R, V>(t, col, keep, t.y0 + j - K, out);
+        if (j >= K && j < K + t.ny) strip_store<R, V>(t, geom, j - K, out);
     };
     for (int st = 0; st < steps; st += 2) {
         step(st, std::integral_constant<int, 0>{});

@@ -45,59 +45,76 @@ struct strip_task {
 
 constexpr unsigned kFullMask = 0xffffffffu;
 
+// What one lane of a warp works on within a strip task.
+template <int V>
+struct lane_geom {
+    int64_t col[V];  // word column of each of the lane's words
+    bool keep[V];    // the lane stores this word (one of the strip's own columns)
+    int src_l;       // lane holding the word left of col[0]
+    int src_r;       // lane holding the word right of col[V-1]
+    int yoff;        // the lane's output rows start at t.y0 + yoff
+    int rows;        // output rows the lane stores (<= t.ny)
+};
+
+// Strip geometry: the warp covers segment words x0-1 .. x0+32V-2 (mod wd);
+// the two end words are halo, neighbours come from the adjacent lanes.
+template <int V>
+__device__ __forceinline__ lane_geom<V> strip_geom(const strip_task& t, int lane) {
+    lane_geom<V> g;
+#pragma unroll
+    for (int i = 0; i < V; ++i) {
+        const int off = V * lane + i;
+        int c = (t.x0 - 1 + off) % t.wd;
+        if (c < 0) c += t.wd;
+        g.col[i] = c;
+        g.keep[i] = off >= 1 && off <= t.nx;
+    }
+    g.src_l = lane > 0 ? lane - 1 : 0;
+    g.src_r = lane < 31 ? lane + 1 : 31;
+    g.yoff = 0;
+    g.rows = t.ny;
+    return g;
+}
+
+// Group geometry for narrow grids (wd <= 16 words, one word per lane): the
+// warp holds `groups` copies of a whole row, each wd lanes wide, with exact
+// toroidal wrap inside a group (no halo words); group q owns output rows
+// t.y0 + q*t.ny .. + t.ny (clipped to the grid).  Lanes past the last group
+// compute a duplicate of group 0's words and store nothing.
+__device__ __forceinline__ lane_geom<1> group_geom(const strip_task& t, int groups, int lane) {
+    lane_geom<1> g;
+    const int wd = t.wd;
+    int q = lane / wd, i = lane - q * wd;
+    const bool live = q < groups;
+    if (!live) q = 0;
+    g.col[0] = i;
+    g.src_l = q * wd + (i == 0 ? wd - 1 : i - 1);
+    g.src_r = q * wd + (i == wd - 1 ? 0 : i + 1);
+    g.yoff = q * t.ny;
+    const int rows_left = t.h - (t.y0 + g.yoff);
+    g.rows = live ? (rows_left < t.ny ? (rows_left > 0 ? rows_left : 0) : t.ny) : 0;
+    g.keep[0] = live;
+    return g;
+}
+
 template <class R, int K, int V>
 struct strip_state {
     uint32_t h[K][2][V][R::NH];  // horizontal aggregates, slot = row parity
     uint32_t c[K][2][V][R::P];   // centre states, slot = row parity
 };
 
-// Pushes one row (level 0) through the K levels.  Q is the parity slot of
-// this row; on return `row` holds the row K rows above it, advanced K
-// generations.
-template <class R, int K, int V, int Q>
-__device__ __forceinline__ void strip_push(strip_state<R, K, V>& s, uint32_t (&row)[V][R::P]) {
-    constexpr int P = R::P, NH = R::NH;
-#pragma unroll
-    for (int g = 0; g < K; ++g) {
-        uint32_t ind[V];
-#pragma unroll
-        for (int i = 0; i < V; ++i) ind[i] = R::indicator(row[i]);
-        const uint32_t lw = __shfl_up_sync(kFullMask, ind[V - 1], 1);
-        const uint32_t rw = __shfl_down_sync(kFullMask, ind[0], 1);
-        uint32_t hc[V][NH];
-#pragma unroll
-        for (int i = 0; i < V; ++i) {
-            const uint32_t l = i == 0 ? lw : ind[i - 1];
-            const uint32_t r = i == V - 1 ? rw : ind[i + 1];
-            R::hagg(west_of(l, ind[i]), ind[i], east_of(ind[i], r), hc[i]);
-        }
-        uint32_t nxt[V][P];
-#pragma unroll
-        for (int i = 0; i < V; ++i) R::next(s.h[g][Q][i], s.h[g][1 - Q][i], hc[i], s.c[g][1 - Q][i], nxt[i]);
-#pragma unroll
-        for (int i = 0; i < V; ++i) {
-#pragma unroll
-            for (int k = 0; k < NH; ++k) s.h[g][Q][i][k] = hc[i][k];
-#pragma unroll
-            for (int p = 0; p < P; ++p) {
-                s.c[g][Q][i][p] = row[i][p];
-                row[i][p] = nxt[i][p];
-            }
-        }
-    }
-}
-
 // One wavefront level: pushes `row` (a row of level g, parity slot Q) into
 // the level's window and returns, in `row`, the row above it advanced one
 // generation.
 template <class R, int K, int V, int Q>
-__device__ __forceinline__ void level_push(strip_state<R, K, V>& s, int g, uint32_t (&row)[V][R::P]) {
+__device__ __forceinline__ void level_push(strip_state<R, K, V>& s, int g, uint32_t (&row)[V][R::P], int src_l,
+                                           int src_r) {
     constexpr int P = R::P, NH = R::NH;
     uint32_t ind[V];
 #pragma unroll
     for (int i = 0; i < V; ++i) ind[i] = R::indicator(row[i]);
-    const uint32_t lw = __shfl_up_sync(kFullMask, ind[V - 1], 1);
-    const uint32_t rw = __shfl_down_sync(kFullMask, ind[0], 1);
+    const uint32_t lw = __shfl_sync(kFullMask, ind[V - 1], src_l);
+    const uint32_t rw = __shfl_sync(kFullMask, ind[0], src_r);
     uint32_t hc[V][NH];
 #pragma unroll
     for (int i = 0; i < V; ++i) {
@@ -120,6 +137,15 @@ __device__ __forceinline__ void level_push(strip_state<R, K, V>& s, int g, uint3
     }
 }
 
+// Pushes one row through the K levels in sequence.  Q is the parity slot of
+// this row; on return `row` holds the row K rows above it, advanced K
+// generations.
+template <class R, int K, int V, int Q>
+__device__ __forceinline__ void strip_push(strip_state<R, K, V>& s, uint32_t (&row)[V][R::P], int src_l, int src_r) {
+#pragma unroll
+    for (int g = 0; g < K; ++g) level_push<R, K, V, Q>(s, g, row, src_l, src_r);
+}
+
 // Skewed wavefront step: level g takes the row level g-1 produced in the
 // previous step (held in pend[g]), so the K levels of one step are
 // independent of each other.  pend[0] is the new input row; on return
@@ -128,11 +154,9 @@ __device__ __forceinline__ void level_push(strip_state<R, K, V>& s, int g, uint3
 // rows alternate parity with the step parity S.
 template <class R, int K, int V, int S>
 __device__ __forceinline__ void skewed_step(strip_state<R, K, V>& s, uint32_t (&pend)[K][V][R::P],
-                                            uint32_t (&out)[V][R::P]) {
+                                            uint32_t (&out)[V][R::P], int src_l, int src_r) {
 #pragma unroll
-    for (int g = 0; g < K; ++g) {
-        level_push<R, K, V, S>(s, g, pend[g]);
-    }
+    for (int g = 0; g < K; ++g) level_push<R, K, V, S>(s, g, pend[g], src_l, src_r);
 #pragma unroll
     for (int i = 0; i < V; ++i)
 #pragma unroll
@@ -145,15 +169,17 @@ __device__ __forceinline__ void skewed_step(strip_state<R, K, V>& s, uint32_t (&
             for (int p = 0; p < R::P; ++p) pend[g][i][p] = pend[g - 1][i][p];
 }
 
+// Stores the lane's words of output row t.y0 + geom.yoff + j (0 <= j < geom.rows).
 template <class R, int V>
-__device__ __forceinline__ void strip_store(const strip_task& t, const int64_t (&col)[V], const bool (&keep)[V],
-                                            int row_idx, const uint32_t (&src)[V][R::P]) {
-    uint32_t* base = t.out + (int64_t)row_idx * t.wd;
+__device__ __forceinline__ void strip_store(const strip_task& t, const lane_geom<V>& geom, int j,
+                                            const uint32_t (&src)[V][R::P]) {
+    if (j >= geom.rows) return;
+    uint32_t* base = t.out + (int64_t)(t.y0 + geom.yoff + j) * t.wd;
 #pragma unroll
     for (int p = 0; p < R::P; ++p)
 #pragma unroll
         for (int i = 0; i < V; ++i)
-            if (keep[i]) base[p * t.plane_words + col[i]] = src[i][p];
+            if (geom.keep[i]) base[p * t.plane_words + geom.col[i]] = src[i][p];
 }
 
 } // namespace cb2

@@ -213,6 +213,61 @@ class DeviceGrid:
         return int(lib.cb2_grid_time_step(self._h))
 
 
+class Batch:
+    """Many device grids advanced together by one persistent kernel (``cb2_batch``).
+
+    ``steps[i]`` generations for ``grids[i]`` per run.  The grids stay owned
+    by the caller and must outlive the batch.
+    """
+
+    def __init__(self, grids: list[DeviceGrid], steps: list[int], temporal_steps: int = 0, tile_rows: int = 0,
+                 spin_limit: int = 0, stall_task: int = -1):
+        if len(grids) != len(steps) or not grids:
+            raise ValueError("grids and steps must be non-empty lists of the same length")
+        self.grids = list(grids)
+        self.steps = [int(s) for s in steps]
+        handles = (ctypes.c_void_p * len(grids))(*[g.handle for g in grids])
+        st = np.ascontiguousarray(self.steps, dtype=np.int64)
+        opts = _abi.BatchOpts(temporal_steps, tile_rows, spin_limit, stall_task)
+        h = ctypes.c_void_p()
+        check(lib.cb2_batch_create(handles, st.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), len(grids),
+                                   ctypes.byref(opts), ctypes.byref(h)), "batch create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.cb2_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, stream=None) -> None:
+        check(lib.cb2_batch_run(self._h, _stream_handle(stream)), "batch run")
+
+    def wait(self, stream=None) -> None:
+        check(lib.cb2_batch_wait(self._h, _stream_handle(stream)), "batch")
+
+    def run_per_grid(self, stream=None) -> None:
+        check(lib.cb2_batch_run_per_grid(self._h, _stream_handle(stream)), "per-grid run")
+
+    def info(self) -> dict:
+        tasks = ctypes.c_int64()
+        cells = ctypes.c_double()
+        ctas = ctypes.c_int()
+        check(lib.cb2_batch_info(self._h, ctypes.byref(tasks), ctypes.byref(cells), ctypes.byref(ctas)))
+        return {"tasks": tasks.value, "cell_updates": cells.value, "persistent_ctas": ctas.value}
+
+
 def plan(automaton, x_size: int, y_size: int, temporal_steps: int = 0, tile_rows: int = 0,
          words_per_lane: int = 0, levels_per_warp: int = 0) -> dict:
     """The plan (temporal depth, strip height, lane width, levels per warp) a run would use."""

@@ -153,6 +153,107 @@ int cb2_grid_planes(cb2_grid* grid, void** planes, int* n_planes, int64_t* words
 /* Generations advanced since the last upload / fill. */
 int64_t cb2_grid_time_step(const cb2_grid* grid);
 
+/* ---- batches: many grids in one persistent kernel ------------------------ */
+/* A batch advances each of its grids by that grid's own number of
+ * generations in one persistent kernel over a queue of strip tasks, replayed
+ * as a captured CUDA graph.  There is no counterpart in the reference, whose
+ * traversers run one grid per launch sequence (traversers/cuda/simple.cuh:44-79);
+ * cb2_batch_run_per_grid is that one-launch-per-grid path over the same grids
+ * for comparison.  The grids stay owned by the caller; while they belong to a
+ * batch, advance them through the batch (a grid advanced or re-uploaded
+ * outside it makes the next cb2_batch_run rebuild the schedule). */
+typedef struct cb2_batch cb2_batch;
+
+typedef struct cb2_batch_opts {
+    int temporal_steps;   /* K of full chunks: 1, 2, 4 or 8 (0 = 8)                  */
+    int tile_rows;        /* output rows per strip task (0 = 256)                      */
+    long long spin_limit; /* iterations a task waits for its grid's previous chunk
+                             before the run fails with CB2_ETIMEOUT (0 = ~4 s)         */
+    int stall_task;       /* test hook: index of a task whose dependency is never
+                             satisfied, to exercise the timeout path (-1 = none)      */
+} cb2_batch_opts;
+
+int cb2_batch_create(cb2_grid* const* grids, const int64_t* steps, int n, const cb2_batch_opts* opts,
+                     cb2_batch** out);
+int cb2_batch_destroy(cb2_batch* batch);
+/* One pass: every grid advances its steps (asynchronous on `stream`). */
+int cb2_batch_run(cb2_batch* batch, void* stream);
+/* Waits for `stream`; CB2_ETIMEOUT if a task's bounded wait ran out. */
+int cb2_batch_wait(cb2_batch* batch, void* stream);
+/* The same work as cb2_batch_run, one launch sequence per grid. */
+int cb2_batch_run_per_grid(cb2_batch* batch, void* stream);
+/* Tasks per run, cell-updates per run, persistent CTAs of the kernel. */
+int cb2_batch_info(const cb2_batch* batch, int64_t* tasks, double* cell_updates, int* persistent_ctas);
+
+/* ---- serving: continuous batching of simulation requests ---------------- */
+/* A server thread admits requests in arrival order while their state fits a
+ * device-memory budget, keeps it resident, and advances every admitted
+ * request by up to chunk_steps generations per round in one persistent batch
+ * kernel; two rounds are in flight at a time, and requests that arrive
+ * meanwhile join at the next round.  No
+ * counterpart in the reference (one process runs one experiment,
+ * experiments/experiment_manager.hpp:43-57).  per_request = 1 runs the plain
+ * path instead: one request at a time, each as one launch sequence. */
+typedef struct cb2_server cb2_server;
+
+typedef struct cb2_server_opts {
+    size_t memory_budget;    /* bytes of request state held at once (0 = min(150 GiB, 80% free)) */
+    int max_active;          /* requests admitted at once (0 = 4096)                    */
+    int chunk_steps;         /* most generations per request per round (0 = 128)       */
+    int temporal_steps;      /* K of the batch kernel: 1, 2, 4 or 8 (0 = 8)            */
+    int tile_rows;           /* output rows per strip task (0 = 128)                   */
+    int per_request;         /* 1 = plain one-request-at-a-time path                   */
+    int task_capacity;       /* strip tasks per round (0 = 2^20)                        */
+    long long spin_limit;    /* bounded wait of a task (0 = ~4 s)                       */
+    long long fail_alloc_at; /* test hook: the n-th state allocation fails (0 = never)  */
+    double round_cells;      /* if > 0: cell-updates a round aims at, shared by its
+                                requests (0 = every request takes chunk_steps)        */
+} cb2_server_opts;
+
+typedef struct cb2_request {
+    int automaton;
+    int64_t x_size, y_size; /* x_size a multiple of 32                                  */
+    int64_t steps;
+    uint64_t seed;          /* seeded input (cb2_grid_fill_random) when host_cells is NULL */
+    int n_thresholds;
+    uint64_t thresholds[7];
+    const uint8_t* host_cells; /* optional input, one dictionary index per cell; read at
+                                  admission, so it must stay valid until then            */
+    uint8_t* host_result;      /* optional output, one index per cell, written at completion */
+} cb2_request;
+
+#define CB2_REQ_QUEUED 0
+#define CB2_REQ_ACTIVE 1
+#define CB2_REQ_DONE 2
+#define CB2_REQ_FAILED 3
+
+typedef struct cb2_request_status {
+    int state;          /* CB2_REQ_*                                   */
+    int error;          /* status code of a failed request             */
+    int64_t steps_done;
+    double submit_s, admit_s, done_s; /* seconds since cb2_server_create */
+    uint64_t checksum[16];            /* of the final generation        */
+} cb2_request_status;
+
+typedef struct cb2_server_stats {
+    int64_t submitted, completed, failed, rounds;
+    double cell_updates;
+    int64_t used_bytes, budget_bytes;
+    double now_s;
+} cb2_server_stats;
+
+int cb2_server_create(const cb2_server_opts* opts, cb2_server** out);
+/* Thread-safe.  CB2_ENOMEM if the request alone exceeds the budget. */
+int cb2_server_submit(cb2_server* server, const cb2_request* request, int64_t* id);
+int cb2_server_status(cb2_server* server, int64_t id, cb2_request_status* status);
+/* Blocks until the request finished (its status code) or CB2_ETIMEOUT. */
+int cb2_server_wait(cb2_server* server, int64_t id, double timeout_s);
+/* Blocks until every submitted request finished, or CB2_ETIMEOUT. */
+int cb2_server_drain(cb2_server* server, double timeout_s);
+int cb2_server_get_stats(cb2_server* server, cb2_server_stats* stats);
+/* Stops the loop; requests not finished are failed. */
+int cb2_server_destroy(cb2_server* server);
+
 /* ---- tuning and measurement --------------------------------------------- */
 /* Times the candidate plans for this automaton and size on the current
  * device, stores the fastest in the in-process tuning table (used whenever a
