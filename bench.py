@@ -5,9 +5,10 @@
 
 A step is one pass of the hot path over one batch: the headline workload
 advances a 65536 x 65536 Game of Life grid (bit planes, 512 MiB packed,
-Bernoulli(0.35) seeded input) by 1000 generations.  Under torchrun each rank
-advances its own grid of that size (independent units, no collective on the
-data path): weak scaling.
+Bernoulli(0.35) seeded input) by 1000 generations.  Under torchrun the grid
+is 65536 wide and N*65536 tall, split into one 65536-row band per rank, with
+a halo exchange of K rows each way between neighbouring ranks (NCCL) before
+every K-generation pass: weak scaling.
 
 value     Gcell-updates/s over all ranks, device-timed (CUDA events on the
           launching stream), inputs resident in HBM, max over ranks.
@@ -354,8 +355,17 @@ def main() -> None:
     tuned = cb.autotune(a, x, y, budget_ms=4000)
     plan = cb.plan(a, x, y)
     k = plan["temporal_steps"]
-    grid = cb.DeviceGrid(a, x, y)
-    grid.fill_random(wl["seed"] + rank, wl["probs"], stream=stream)
+    if world == 1:
+        grid = cb.DeviceGrid(a, x, y)
+        grid.fill_random(wl["seed"], wl["probs"], stream=stream)
+    else:
+        # one grid of world*y rows split into bands, one per rank (NCCL halo exchange per pass)
+        from cellato_b200.bands import BandGrid
+
+        cb.autotune(a, x, y, budget_ms=4000)
+        grid = BandGrid(a, x, y * world, rank, world)
+        grid.fill_random(wl["seed"], wl["probs"], stream=stream)
+        k = grid.plan_k()
 
     def barrier():
         if world > 1:
@@ -423,25 +433,37 @@ def main() -> None:
         "generations_per_launch": gens_per_launch,
     }
 
-    # ---- end to end through the C-ABI with host buffers ----
+    # ---- end to end through the public API with host buffers ----
     nbytes = cb.layout_bytes(a, "bit_planes", 64, x, y)
     host_in = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
     host_out = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
-    grid.download("bit_planes", 64, stream=stream, out=host_in.numpy())
-    host_img = cb.HostGrid(a, "bit_planes", 64, x, y, host_in.numpy())
-    for _ in range(1):
-        grid.upload(host_img, stream=stream)
-        grid.run(gens, stream=stream)
-        grid.download("bit_planes", 64, stream=stream, out=host_out.numpy())
+    if world == 1:
+        grid.download("bit_planes", 64, stream=stream, out=host_in.numpy())
+        host_img = cb.HostGrid(a, "bit_planes", 64, x, y, host_in.numpy())
+
+        def e2e_step():
+            grid.upload(host_img, stream=stream)
+            grid.run(gens, stream=stream)
+            grid.download("bit_planes", 64, stream=stream, out=host_out.numpy())
+    else:
+        g0, nb = grid.ghost, grid.band
+        band_in = host_in.view(torch.int32).view(P, nb, x // 32)
+        band_out = host_out.view(torch.int32).view(P, nb, x // 32)
+        band_in.copy_(grid.planes[:, g0:g0 + nb])
+
+        def e2e_step():
+            grid.planes[:, g0:g0 + nb].copy_(band_in, non_blocking=True)
+            grid.run(gens, stream=stream)
+            band_out.copy_(grid.planes[:, g0:g0 + nb], non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+    e2e_step()
     torch.cuda.synchronize()
     barrier()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     w0 = time.perf_counter()
     f0.record(stream)
     for _ in range(args.steps):
-        grid.upload(host_img, stream=stream)
-        grid.run(gens, stream=stream)
-        grid.download("bit_planes", 64, stream=stream, out=host_out.numpy())
+        e2e_step()
     f1.record(stream)
     f1.synchronize()
     wall = time.perf_counter() - w0
@@ -450,11 +472,14 @@ def main() -> None:
     e2e_wall = max_over_ranks(wall)
     e2e_value = world * cells * gens * args.steps / (e2e_ms * 1e-3) / 1e9
 
+    if world == 1:
+        grid.close()
+    else:
+        del grid
+    torch.cuda.synchronize()
     batched = None
     if not args.no_batch:
-        grid.close()
         batched = bench_batch(cb, torch, stream, args.batch_grids, max(3, args.steps))
-        grid = cb.DeviceGrid(a, x, y)
     served = None
     if not args.no_serve:
         served = bench_serve(cb, args.serve_requests, [100.0, 1000.0, 5000.0, 20000.0])
@@ -463,7 +488,6 @@ def main() -> None:
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_sample(a, wl["probs"], args.cpu_seconds)
 
-    grid.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -476,11 +500,14 @@ def main() -> None:
         "config": {"workload": wl["desc"], "automaton": name, "x_size": x, "y_size": y,
                    "generations_per_step": gens, "plan": plan, "autotuned": tuned,
                    "l2": "inputs larger than L2 (each plane buffer is 512 MiB at 65536^2)",
-                   "parallelism": f"replicas x{world} (one grid per GPU)" if world > 1 else "single GPU"},
+                   "parallelism": (f"row bands x{world}: one {x}x{y * world} grid, {y} rows per GPU, NCCL halo "
+                                   f"exchange of K rows each way per pass" if world > 1 else "single GPU")},
         "roofline": roof,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-                "wall_s": e2e_wall, "path": "cb2_grid_upload(bit_planes) + cb2_grid_run + cb2_grid_download, "
-                                            "pinned host buffers"},
+                "wall_s": e2e_wall,
+                "path": ("cb2_grid_upload(bit_planes) + cb2_grid_run + cb2_grid_download, pinned host buffers"
+                         if world == 1 else "band planes from pinned host memory + BandGrid.run (halo exchange + "
+                                            "cb2_band_pass per pass) + band planes back, per rank")},
         "gpu_launches": launches,
         "clocks": clocks,
         "cpu_baseline": cpu,

@@ -107,6 +107,11 @@ _SIGNATURES = {
     "cb2_run_bit_planes": (ctypes.c_int, [ctypes.c_int, _vpp, _vpp, _i64, _i64, _i64, _tp, _vp,
                                           ctypes.POINTER(ctypes.c_int)]),
     "cb2_run_bit_planes_in_place": (ctypes.c_int, [ctypes.c_int, _vpp, _i64, _i64, _i64, _tp, _vp]),
+    "cb2_band_pass": (ctypes.c_int, [ctypes.c_int, _vpp, _vpp, _i64, _i64, _i64, _i64, ctypes.c_int, _tp, _vp]),
+    "cb2_fill_random_planes": (ctypes.c_int, [ctypes.c_int, _vpp, _i64, _i64, _i64, _i64, ctypes.c_uint64, _u64p,
+                                              ctypes.c_int, _vp]),
+    "cb2_checksum_planes": (ctypes.c_int, [ctypes.c_int, _vpp, _i64, _i64, _i64, _i64, _i64, _i64, _i64p,
+                                           ctypes.c_int, _u64p, _vp]),
     "cb2_grid_create": (ctypes.c_int, [ctypes.c_int, _i64, _i64, ctypes.POINTER(_vp)]),
     "cb2_grid_destroy": (ctypes.c_int, [_vp]),
     "cb2_grid_upload": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_size_t, _vp]),

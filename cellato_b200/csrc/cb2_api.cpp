@@ -99,7 +99,7 @@ static bool valid_k(int k) { return k == 1 || k == 2 || k == 4 || k == 8 || k ==
 static const int kDefaultPlan[kNumAutomata][3] = {{8, 1, 8}, {16, 2, 2}, {16, 1, 16}};
 
 // Fills every 0 field of `t` for a grid of geometry g.
-static int resolve_plan(const grid_geom& g, const cb2_tuning* t, run_plan* plan) {
+int resolve_plan(const grid_geom& g, const cb2_tuning* t, run_plan* plan) {
     cb2_tuning want{0, 0, 0, 0};
     if (t) want = *t;
     cb2_tuning tuned{0, 0, 0, 0};

@@ -1,0 +1,130 @@
+// cb2_band.cpp -- entry points for a grid split into row bands across GPUs.
+//
+// Each rank holds its band of rows plus `ghost` rows above and below in
+// caller-owned planes (rows_total = band + 2 * ghost).  Before a pass of K
+// generations (K <= ghost), the K ghost rows next to the band are refreshed
+// from the neighbouring ranks (a halo exchange the caller runs, e.g. NCCL
+// send/recv of contiguous rows); the pass then writes only the band's rows,
+// reading the ghosts for the rows it needs outside the band.  The seeded
+// input and the checksum are defined on the global grid, so a band run gives
+// the same cells and the same 16 tile sums as one grid of the global size.
+#include "cellato_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "cb2_internal.h"
+
+namespace cb2 {
+namespace {
+
+int check_planes(const grid_geom& g, const void* const* planes, const char* what) {
+    if (!planes) {
+        set_error(std::string("null ") + what + " plane array");
+        return CB2_EINVAL;
+    }
+    for (int p = 1; p < g.planes; ++p)
+        if ((const char*)planes[p] - (const char*)planes[0] != (ptrdiff_t)(p * g.plane_words * 4)) {
+            set_error(std::string(what) + " planes must be consecutive in one allocation (stride = rows * x_size / 8 bytes)");
+            return CB2_EINVAL;
+        }
+    return CB2_OK;
+}
+
+int cuda_err(cudaError_t e, const char* what) {
+    cudaGetLastError();
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return CB2_ECUDA;
+}
+
+} // namespace
+} // namespace cb2
+
+using namespace cb2;
+
+extern "C" {
+
+int cb2_band_pass(int automaton, void* const* in, void* const* out, int64_t x_size, int64_t rows_total,
+                  int64_t row_first, int64_t rows_out, int temporal_steps, const cb2_tuning* tuning, void* stream) {
+    grid_geom g;
+    int rc = make_geom(automaton, x_size, rows_total, &g);
+    if (rc) return rc;
+    if ((rc = check_planes(g, in, "input")) || (rc = check_planes(g, out, "output"))) return rc;
+    if (row_first < 0 || rows_out < 1 || row_first + rows_out > rows_total) {
+        set_error("band rows outside the planes");
+        return CB2_EINVAL;
+    }
+    if (row_first < temporal_steps || rows_total - (row_first + rows_out) < temporal_steps) {
+        set_error("a pass of " + std::to_string(temporal_steps) + " generations needs that many ghost rows each side");
+        return CB2_EINVAL;
+    }
+    cb2_tuning t{temporal_steps, 0, 0, 0};
+    if (tuning) {
+        t = *tuning;
+        t.temporal_steps = temporal_steps;
+    }
+    grid_geom window = g;  // plan the tiles for the band's rows
+    window.h = (int32_t)rows_out;
+    window.y_size = rows_out;
+    window.plane_words = (int64_t)g.wd * rows_out;
+    run_plan plan;
+    rc = resolve_plan(window, &t, &plan);
+    if (rc) return rc;
+    cudaError_t e = launch_strip_window(g, (const uint32_t*)in[0], (uint32_t*)out[0], plan, (int)row_first,
+                                        (int)rows_out, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_err(e, "band pass launch");
+    return CB2_OK;
+}
+
+int cb2_fill_random_planes(int automaton, void* const* planes, int64_t x_size, int64_t rows, int64_t global_row0,
+                           int64_t global_rows, uint64_t seed, const uint64_t* thresholds, int n_thresholds,
+                           void* stream) {
+    grid_geom g;
+    int rc = make_geom(automaton, x_size, rows, &g);
+    if (rc) return rc;
+    if ((rc = check_planes(g, planes, "output"))) return rc;
+    if (global_rows < 1 || n_thresholds < 0 || n_thresholds > kMaxThresholds || n_thresholds >= (1 << g.planes) ||
+        (n_thresholds && !thresholds)) {
+        set_error("invalid global rows or thresholds");
+        return CB2_EINVAL;
+    }
+    cudaError_t e = launch_fill_random_rows(g, (uint32_t*)planes[0], seed, thresholds, n_thresholds, global_row0,
+                                            global_rows, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_err(e, "fill launch");
+    return CB2_OK;
+}
+
+int cb2_checksum_planes(int automaton, const void* const* planes, int64_t x_size, int64_t rows, int64_t row_first,
+                        int64_t row_count, int64_t global_row0, int64_t global_rows, const int64_t* values,
+                        int n_values, uint64_t out[16], void* stream) {
+    grid_geom g;
+    int rc = make_geom(automaton, x_size, rows, &g);
+    if (rc) return rc;
+    if ((rc = check_planes(g, planes, "input"))) return rc;
+    if (!out || n_values < 0 || n_values > (1 << kMaxPlanes) || (n_values && !values)) {
+        set_error("null output or more than 8 state values");
+        return CB2_EINVAL;
+    }
+    if (row_first < 0 || row_count < 0 || row_first + row_count > rows || global_row0 < 0 ||
+        global_row0 + row_count > global_rows) {
+        set_error("checksum rows outside the planes or the global grid");
+        return CB2_EINVAL;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned long long* sums = nullptr;
+    cudaError_t e = cudaMallocAsync(&sums, 16 * sizeof(unsigned long long), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(sums, 0, 16 * sizeof(unsigned long long), s);
+    if (e == cudaSuccess)
+        e = launch_checksum_rows(g, (const uint32_t*)planes[0], values, values ? n_values : 0, row_first, row_count,
+                                 global_row0, global_rows, sums, s);
+    unsigned long long host[16] = {};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host, sums, sizeof(host), cudaMemcpyDeviceToHost, s);
+    if (sums) cudaFreeAsync(sums, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_err(e, "band checksum");
+    for (int i = 0; i < 16; ++i) out[i] = host[i];
+    return CB2_OK;
+}
+
+} // extern "C"

@@ -47,6 +47,9 @@ int find_automaton(const char* name);
 // Launches one K-generation strip pass over a whole grid (in -> out).
 cudaError_t launch_strip_pass(const grid_geom& g, const uint32_t* in, uint32_t* out, const run_plan& plan,
                               cudaStream_t stream);
+// The same for output rows [y_base, y_base + rows_out) only (input rows wrap mod g.h).
+cudaError_t launch_strip_window(const grid_geom& g, const uint32_t* in, uint32_t* out, const run_plan& plan,
+                                int y_base, int rows_out, cudaStream_t stream);
 // Strip tasks per column and per row for a plan.
 void strip_counts(const grid_geom& g, int v, int tile_rows, int* nsx, int* nsy);
 // The instantiated kernels of an automaton, and the first one matching a
@@ -73,9 +76,17 @@ cudaError_t launch_planes_to_tiled(const grid_geom& g, const uint32_t* planes, v
                                    cudaStream_t s);
 cudaError_t launch_fill_random(const grid_geom& g, uint32_t* planes, uint64_t seed, const uint64_t* thr, int nthr,
                                cudaStream_t s);
+// Row y of the planes gets global row (row0 + y) mod global_rows of the seeded grid.
+cudaError_t launch_fill_random_rows(const grid_geom& g, uint32_t* planes, uint64_t seed, const uint64_t* thr, int nthr,
+                                    int64_t row0, int64_t global_rows, cudaStream_t s);
 // Adds the 16 tile sums of state values into sums[16] (which the caller zeroes).
 cudaError_t launch_checksum(const grid_geom& g, const uint32_t* planes, const int64_t* values, int nvalues,
                             unsigned long long* sums, cudaStream_t s);
+// The same for rows [row_first, row_first + row_count), which are global rows
+// global_row0.. of a grid global_rows tall (a band's share of the global tiles).
+cudaError_t launch_checksum_rows(const grid_geom& g, const uint32_t* planes, const int64_t* values, int nvalues,
+                                 int64_t row_first, int64_t row_count, int64_t global_row0, int64_t global_rows,
+                                 unsigned long long* sums, cudaStream_t s);
 
 // Integer-pipe peak probe: `iters` rounds of independent 3-input logic ops.
 cudaError_t launch_lop3_probe(uint32_t* sink, int blocks, int threads, int iters, cudaStream_t s);
@@ -93,6 +104,9 @@ namespace cb2 {
 
 // Validates a grid size for an automaton and fills its geometry.
 int make_geom(int automaton, int64_t x, int64_t y, grid_geom* g);
+// The run plan for a grid: the fields of `t` that are 0 are chosen from the
+// tuning table or the defaults.
+int resolve_plan(const grid_geom& g, const cb2_tuning* t, run_plan* plan);
 // Launches `steps` generations starting in bufs[cur], alternating between the
 // two buffers; *result is the index of the buffer holding the result.
 int run_chunks(const grid_geom& g, uint32_t* const bufs[2], int cur, int64_t steps, const cb2_tuning* tuning,

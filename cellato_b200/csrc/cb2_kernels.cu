@@ -31,6 +31,7 @@ struct strip_launch {
     int64_t plane_words;
     int32_t wd, h;
     int32_t nsx, nsy, tile_rows;
+    int32_t y_base, rows_out;  // output rows [y_base, y_base + rows_out)
 };
 
 template <class R, int K, int V, int L>
@@ -47,8 +48,8 @@ __global__ void __launch_bounds__(32 * (K / L)) pipe_kernel(strip_launch a) {
     t.h = a.h;
     t.x0 = sx * own;
     t.nx = min(own, a.wd - t.x0);
-    t.y0 = sy * a.tile_rows;
-    t.ny = min(a.tile_rows, a.h - t.y0);
+    t.y0 = a.y_base + sy * a.tile_rows;
+    t.ny = min(a.tile_rows, a.y_base + a.rows_out - t.y0);
     if constexpr (L == K)
         warp_run<R, K, V, kRingDepth>(t, strip_geom<V>(t, threadIdx.x & 31), smem);  // one warp, skewed levels
     else
@@ -146,10 +147,10 @@ int auto_tile_rows(const grid_geom& g, const strip_variant& sv) {
     return std::min(rows, (int)g.h);
 }
 
-cudaError_t launch_strip_pass(const grid_geom& g, const uint32_t* in, uint32_t* out, const run_plan& plan,
-                              cudaStream_t stream) {
+cudaError_t launch_strip_window(const grid_geom& g, const uint32_t* in, uint32_t* out, const run_plan& plan,
+                                int y_base, int rows_out, cudaStream_t stream) {
     const strip_variant* sv = find_variant(g.automaton, plan.k, plan.v, plan.l);
-    if (!sv) return cudaErrorInvalidValue;
+    if (!sv || rows_out < 1 || y_base < 0 || y_base + rows_out > g.h) return cudaErrorInvalidValue;
     resident_strip_tasks(*sv);  // sets the kernel's shared-memory attribute once
     strip_launch a;
     a.in = in;
@@ -158,10 +159,19 @@ cudaError_t launch_strip_pass(const grid_geom& g, const uint32_t* in, uint32_t* 
     a.wd = g.wd;
     a.h = g.h;
     a.tile_rows = plan.tile_rows;
-    strip_counts(g, plan.v, plan.tile_rows, &a.nsx, &a.nsy);
+    a.y_base = y_base;
+    a.rows_out = rows_out;
+    grid_geom window = g;
+    window.h = rows_out;
+    strip_counts(window, plan.v, plan.tile_rows, &a.nsx, &a.nsy);
     const int64_t tasks = (int64_t)a.nsx * a.nsy;
     void* args[] = {&a};
     return cudaLaunchKernel(sv->fn, dim3((unsigned)tasks), dim3(sv->threads), args, (size_t)sv->smem_bytes, stream);
+}
+
+cudaError_t launch_strip_pass(const grid_geom& g, const uint32_t* in, uint32_t* out, const run_plan& plan,
+                              cudaStream_t stream) {
+    return launch_strip_window(g, in, out, plan, 0, g.h, stream);
 }
 
 // ---------------------------------------------------------------------------
@@ -181,12 +191,15 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
     return z ^ (z >> 31);
 }
 
+// Row y of the planes holds global row (row0 + y) mod global_rows.
 __global__ void fill_random_kernel(uint32_t* planes, int64_t plane_words, int32_t wd, int64_t x_size, int P,
-                                   uint64_t seed, thr_pack thr) {
+                                   uint64_t seed, thr_pack thr, int64_t row0, int64_t global_rows) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < plane_words; w += stride) {
         const int64_t y = w / wd, xw = w - y * wd;
-        const uint64_t i0 = (uint64_t)(y * x_size + xw * 32);
+        int64_t gy = (row0 + y) % global_rows;
+        if (gy < 0) gy += global_rows;
+        const uint64_t i0 = (uint64_t)(gy * x_size + xw * 32);
         uint32_t out[kMaxPlanes] = {0, 0, 0};
 #pragma unroll 4
         for (int j = 0; j < 32; ++j) {
@@ -205,15 +218,20 @@ static unsigned grid_for(int64_t items, int threads) {
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 64));
 }
 
-cudaError_t launch_fill_random(const grid_geom& g, uint32_t* planes, uint64_t seed, const uint64_t* thr, int nthr,
-                               cudaStream_t s) {
-    if (nthr < 0 || nthr > kMaxThresholds) return cudaErrorInvalidValue;
+cudaError_t launch_fill_random_rows(const grid_geom& g, uint32_t* planes, uint64_t seed, const uint64_t* thr, int nthr,
+                                    int64_t row0, int64_t global_rows, cudaStream_t s) {
+    if (nthr < 0 || nthr > kMaxThresholds || global_rows < 1) return cudaErrorInvalidValue;
     thr_pack tp{};
     for (int i = 0; i < nthr; ++i) tp.t[i] = thr[i];
     tp.n = nthr;
     fill_random_kernel<<<grid_for(g.plane_words, 256), 256, 0, s>>>(planes, g.plane_words, g.wd, g.x_size, g.planes,
-                                                                     seed, tp);
+                                                                     seed, tp, row0, global_rows);
     return cudaGetLastError();
+}
+
+cudaError_t launch_fill_random(const grid_geom& g, uint32_t* planes, uint64_t seed, const uint64_t* thr, int nthr,
+                               cudaStream_t s) {
+    return launch_fill_random_rows(g, planes, seed, thr, nthr, 0, g.h, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -446,18 +464,22 @@ struct value_pack {
     long long v[1 << kMaxPlanes];
 };
 
+// Sums rows [row_first, row_first + row_count) of the planes, which are
+// global rows global_row0 + (y - row_first) of a grid global_rows tall.
 __global__ void checksum_kernel(const uint32_t* __restrict__ planes, int64_t plane_words, int32_t wd,
-                                int64_t x_size, int64_t y_size, int P, value_pack vals,
-                                unsigned long long* sums) {
+                                int64_t x_size, int64_t row_first, int64_t row_count, int64_t global_row0,
+                                int64_t global_rows, int P, value_pack vals, unsigned long long* sums) {
     __shared__ unsigned long long acc[16];
     if (threadIdx.x < 16) acc[threadIdx.x] = 0;
     __syncthreads();
-    const int64_t tw = (x_size + 3) / 4, th = (y_size + 3) / 4;
+    const int64_t tw = (x_size + 3) / 4, th = (global_rows + 3) / 4;
     const int nstates = 1 << P;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < plane_words; w += stride) {
-        const int64_t y = w / wd, xw = w - y * wd;
-        const int ty = (int)(y / th);
+    const int64_t words = row_count * wd;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < words; k += stride) {
+        const int64_t yr = k / wd, xw = k - yr * wd;
+        const int64_t w = (row_first + yr) * wd + xw;
+        const int ty = (int)((global_row0 + yr) / th);
         uint32_t in[kMaxPlanes] = {0, 0, 0};
         for (int p = 0; p < P; ++p) in[p] = planes[p * plane_words + w];
         const int64_t x0 = xw * 32, x1 = x0 + 32;
@@ -478,13 +500,23 @@ __global__ void checksum_kernel(const uint32_t* __restrict__ planes, int64_t pla
     if (threadIdx.x < 16 && acc[threadIdx.x]) atomicAdd(&sums[threadIdx.x], acc[threadIdx.x]);
 }
 
-cudaError_t launch_checksum(const grid_geom& g, const uint32_t* planes, const int64_t* values, int nvalues,
-                            unsigned long long* sums, cudaStream_t s) {
+cudaError_t launch_checksum_rows(const grid_geom& g, const uint32_t* planes, const int64_t* values, int nvalues,
+                                 int64_t row_first, int64_t row_count, int64_t global_row0, int64_t global_rows,
+                                 unsigned long long* sums, cudaStream_t s) {
+    if (row_first < 0 || row_count < 0 || row_first + row_count > g.h || global_row0 < 0 ||
+        global_row0 + row_count > global_rows)
+        return cudaErrorInvalidValue;
     value_pack vp{};
     for (int i = 0; i < (1 << kMaxPlanes); ++i) vp.v[i] = i < nvalues ? values[i] : i;
-    checksum_kernel<<<grid_for(g.plane_words, 256), 256, 0, s>>>(planes, g.plane_words, g.wd, g.x_size, g.y_size,
-                                                                 g.planes, vp, sums);
+    checksum_kernel<<<grid_for(row_count * g.wd, 256), 256, 0, s>>>(planes, g.plane_words, g.wd, g.x_size, row_first,
+                                                                    row_count, global_row0, global_rows, g.planes, vp,
+                                                                    sums);
     return cudaGetLastError();
+}
+
+cudaError_t launch_checksum(const grid_geom& g, const uint32_t* planes, const int64_t* values, int nvalues,
+                            unsigned long long* sums, cudaStream_t s) {
+    return launch_checksum_rows(g, planes, values, nvalues, 0, g.h, 0, g.h, sums, s);
 }
 
 // ---------------------------------------------------------------------------

@@ -153,6 +153,31 @@ int cb2_grid_planes(cb2_grid* grid, void** planes, int* n_planes, int64_t* words
 /* Generations advanced since the last upload / fill. */
 int64_t cb2_grid_time_step(const cb2_grid* grid);
 
+/* ---- row bands: one grid split across GPUs -------------------------------- */
+/* A rank holds its band of rows plus `ghost` rows above and below in
+ * caller-owned planes (rows_total = band rows + 2 * ghost, P consecutive
+ * planes).  Before each pass the caller refreshes the ghost rows next to the
+ * band from the neighbouring ranks (a halo exchange of contiguous rows, e.g.
+ * NCCL send/recv); the pass then advances exactly `temporal_steps`
+ * generations of rows [row_first, row_first + rows_out) from in to out,
+ * reading up to temporal_steps rows outside them.  The reference runs one
+ * grid on one GPU (traversers/cuda/temporal.cuh:153-245); this is the
+ * multi-GPU split of that run. */
+int cb2_band_pass(int automaton, void* const* in, void* const* out, int64_t x_size, int64_t rows_total,
+                  int64_t row_first, int64_t rows_out, int temporal_steps, const cb2_tuning* tuning, void* stream);
+/* Seeded input (cb2_grid_fill_random's stream) for caller-owned planes whose
+ * row y is global row (global_row0 + y) mod global_rows of the global grid. */
+int cb2_fill_random_planes(int automaton, void* const* planes, int64_t x_size, int64_t rows, int64_t global_row0,
+                           int64_t global_rows, uint64_t seed, const uint64_t* thresholds, int n_thresholds,
+                           void* stream);
+/* The 16 tile sums (memory/standard_grid.hpp:182-218) contributed by rows
+ * [row_first, row_first + row_count) of the planes, which are global rows
+ * global_row0.. of a grid global_rows tall; summing the results of all
+ * bands gives the global checksum.  Synchronises `stream`. */
+int cb2_checksum_planes(int automaton, const void* const* planes, int64_t x_size, int64_t rows, int64_t row_first,
+                        int64_t row_count, int64_t global_row0, int64_t global_rows, const int64_t* values,
+                        int n_values, uint64_t out[16], void* stream);
+
 /* ---- batches: many grids in one persistent kernel ------------------------ */
 /* A batch advances each of its grids by that grid's own number of
  * generations in one persistent kernel over a queue of strip tasks, replayed
