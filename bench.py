@@ -411,8 +411,8 @@ def main() -> None:
     int_gops = int_ops_per_launch / avg_launch_s / 1e9
     int_frac = int_gops / (lop3_peak / 1e9)
     hbm_frac = hbm_gbs / hbm_peak
-    kernel_key = (f"pipe_kernel<{name},K={k},V={plan['words_per_lane']},L={plan['levels_per_warp']}>"
-                  f"@{x}x{y}")
+    kernel_key = (f"pipe_kernel<{name},K={k},V={plan['words_per_lane']},L={plan['levels_per_warp']},"
+                  f"R={plan['rows_per_step']}>@{x}x{y}")
     traffic = traffic_for(kernel_key)
     roof = {
         "bound": "int" if int_frac >= hbm_frac else "hbm",

@@ -7,12 +7,13 @@ run_params surface.  Importing it without the built library raises.
 """
 from ._abi import CudaError, StateError, last_error
 from .grid import (AUTOMATA, Batch, DeviceGrid, HostGrid, autotune, automaton_id, automaton_info, layout_bytes,
-                   measure_lop3_peak, network_ops, plan, run_bit_planes, thresholds, tuning_load, tuning_save)
+                   measure_lop3_peak, network_ops, plan, run_bit_planes, thresholds, tuning_load, tuning_save,
+                   variants)
 from .serve import Server
 from .traverser import RunParams, Traverser, run_experiment
 
 __all__ = [
     "AUTOMATA", "Batch", "CudaError", "DeviceGrid", "HostGrid", "RunParams", "Server", "StateError", "Traverser", "autotune",
     "automaton_id", "automaton_info", "last_error", "layout_bytes", "measure_lop3_peak", "network_ops", "plan",
-    "run_bit_planes", "run_experiment", "thresholds", "tuning_load", "tuning_save",
+    "run_bit_planes", "run_experiment", "thresholds", "tuning_load", "tuning_save", "variants",
 ]

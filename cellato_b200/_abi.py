@@ -50,11 +50,12 @@ class StateError(ValueError):
 
 class Tuning(ctypes.Structure):
     _fields_ = [("temporal_steps", ctypes.c_int), ("tile_rows", ctypes.c_int), ("words_per_lane", ctypes.c_int),
-                ("levels_per_warp", ctypes.c_int)]
+                ("levels_per_warp", ctypes.c_int), ("rows_per_step", ctypes.c_int)]
 
     def as_dict(self):
         return {"temporal_steps": self.temporal_steps, "tile_rows": self.tile_rows,
-                "words_per_lane": self.words_per_lane, "levels_per_warp": self.levels_per_warp}
+                "words_per_lane": self.words_per_lane, "levels_per_warp": self.levels_per_warp,
+                "rows_per_step": self.rows_per_step}
 
 
 class BatchOpts(ctypes.Structure):
@@ -139,6 +140,7 @@ _SIGNATURES = {
     "cb2_tuning_load": (ctypes.c_int, [ctypes.c_char_p]),
     "cb2_tuning_save": (ctypes.c_int, [ctypes.c_char_p]),
     "cb2_plan": (ctypes.c_int, [ctypes.c_int, _i64, _i64, _tp, _tp]),
+    "cb2_variants": (ctypes.c_int, [ctypes.c_int, _tp, ctypes.c_int]),
     "cb2_measure_lop3_peak": (ctypes.c_int, [ctypes.POINTER(ctypes.c_double)]),
     "cb2_network_ops": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                        ctypes.POINTER(ctypes.c_double)]),
@@ -191,5 +193,6 @@ def declared_symbols() -> list[str]:
     return sorted(set(re.findall(r"\b(cb2_[a-z0-9_]+)\s*\(", text)))
 
 
-def tuning(temporal_steps: int = 0, tile_rows: int = 0, words_per_lane: int = 0, levels_per_warp: int = 0) -> Tuning:
-    return Tuning(temporal_steps, tile_rows, words_per_lane, levels_per_warp)
+def tuning(temporal_steps: int = 0, tile_rows: int = 0, words_per_lane: int = 0, levels_per_warp: int = 0,
+           rows_per_step: int = 0) -> Tuning:
+    return Tuning(temporal_steps, tile_rows, words_per_lane, levels_per_warp, rows_per_step)

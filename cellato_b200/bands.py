@@ -25,7 +25,7 @@ from . import _abi
 from ._abi import check, lib
 from .grid import automaton_id, automaton_info, plan, thresholds
 
-GHOST = 16  # rows kept on each side: the largest temporal depth
+GHOST = 32  # rows kept on each side: the largest temporal depth
 
 
 def exchange_halos(planes: torch.Tensor, ghost: int, band_rows: int, k: int, rank: int, world: int,

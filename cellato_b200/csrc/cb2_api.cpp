@@ -92,21 +92,22 @@ static bool tuned_entry(int automaton, int64_t x, int64_t y, cb2_tuning* out) {
     return false;
 }
 
-static bool valid_k(int k) { return k == 1 || k == 2 || k == 4 || k == 8 || k == 16; }
+static bool valid_k(int k) { return k == 1 || k == 2 || k == 4 || k == 8 || k == 16 || k == 32; }
 
-// Default (K, V, L) per automaton, the fastest plans measured on B200 at the
-// headline sizes; cb2_autotune replaces them per size.
-static const int kDefaultPlan[kNumAutomata][3] = {{8, 1, 8}, {16, 2, 2}, {16, 1, 16}};
+// Default (K, V, L, rows per step) per automaton, the fastest plans measured
+// on B200 at the headline sizes; cb2_autotune replaces them per size.
+static const int kDefaultPlan[kNumAutomata][4] = {{32, 2, 16, 4}, {32, 1, 16, 4}, {32, 2, 16, 4}};
 
 // Fills every 0 field of `t` for a grid of geometry g.
 int resolve_plan(const grid_geom& g, const cb2_tuning* t, run_plan* plan) {
-    cb2_tuning want{0, 0, 0, 0};
+    cb2_tuning want{0, 0, 0, 0, 0};
     if (t) want = *t;
-    cb2_tuning tuned{0, 0, 0, 0};
+    cb2_tuning tuned{0, 0, 0, 0, 0};
     const bool have_tuned = tuned_entry(g.automaton, g.x_size, g.y_size, &tuned);
     const int* def = kDefaultPlan[g.automaton];
     const int k = want.temporal_steps ? want.temporal_steps : (have_tuned ? tuned.temporal_steps : def[0]);
-    if (!valid_k(k)) return fail(CB2_EINVAL, "temporal_steps must be 1, 2, 4, 8 or 16 (got " + std::to_string(k) + ")");
+    if (!valid_k(k))
+        return fail(CB2_EINVAL, "temporal_steps must be 1, 2, 4, 8, 16 or 32 (got " + std::to_string(k) + ")");
     const bool tuned_k = have_tuned && tuned.temporal_steps == k;
     int v = want.words_per_lane;
     if (!v) v = tuned_k ? tuned.words_per_lane : (g.wd <= 30 ? 1 : (k == def[0] ? def[1] : 2));
@@ -114,18 +115,29 @@ int resolve_plan(const grid_geom& g, const cb2_tuning* t, run_plan* plan) {
         return fail(CB2_EINVAL, "words_per_lane must be 1, 2 or 4 (got " + std::to_string(v) + ")");
     int l = want.levels_per_warp;
     if (!l) l = (tuned_k && tuned.words_per_lane == v) ? tuned.levels_per_warp : (k == def[0] && v == def[1] ? def[2] : 0);
-    const strip_variant* sv = find_variant(g.automaton, k, v, l);
-    if (!sv && !want.levels_per_warp) sv = find_variant(g.automaton, k, v, 0);
+    int r = want.rows_per_step;
+    if (r && r != 1 && r != 2 && r != 4)
+        return fail(CB2_EINVAL, "rows_per_step must be 1, 2 or 4 (got " + std::to_string(r) + ")");
+    if (!r)
+        r = (tuned_k && tuned.words_per_lane == v && tuned.levels_per_warp == l)
+                ? tuned.rows_per_step
+                : (k == def[0] && v == def[1] && l == def[2] ? def[3] : 0);
+    const strip_variant* sv = find_variant(g.automaton, k, v, l, r);
+    if (!sv && !want.levels_per_warp && !want.rows_per_step) sv = find_variant(g.automaton, k, v, 0);
     if (!sv)
         return fail(CB2_EINVAL, "no strip kernel for temporal_steps=" + std::to_string(k) + ", words_per_lane=" +
-                                    std::to_string(v) + ", levels_per_warp=" + std::to_string(l));
+                                    std::to_string(v) + ", levels_per_warp=" + std::to_string(l) +
+                                    ", rows_per_step=" + std::to_string(r));
     int rows = want.tile_rows;
-    if (!rows && tuned_k && tuned.words_per_lane == sv->v && tuned.levels_per_warp == sv->l) rows = tuned.tile_rows;
+    if (!rows && tuned_k && tuned.words_per_lane == sv->v && tuned.levels_per_warp == sv->l &&
+        tuned.rows_per_step == sv->r)
+        rows = tuned.tile_rows;
     if (!rows) rows = auto_tile_rows(g, *sv);
     if (rows < 1) return fail(CB2_EINVAL, "tile_rows must be positive");
     plan->k = sv->k;
     plan->v = sv->v;
     plan->l = sv->l;
+    plan->r = sv->r;
     plan->tile_rows = std::min(rows, (int)g.h);
     return CB2_OK;
 }
@@ -159,7 +171,7 @@ int run_chunks(const grid_geom& g, uint32_t* const bufs[2], int cur, int64_t ste
         if (left < p.k) {  // remainder in powers of two, same lane width where possible
             int k = 1;
             while (k * 2 <= left) k *= 2;
-            cb2_tuning t2{k, 0, p.v, 0};
+            cb2_tuning t2{k, 0, p.v, 0, 0};
             if (!find_variant(g.automaton, k, p.v, 0)) t2.words_per_lane = 0;
             rc = resolve_plan(g, &t2, &p);
             if (rc) return rc;
@@ -420,8 +432,16 @@ int cb2_plan(int automaton, int64_t x_size, int64_t y_size, const cb2_tuning* tu
     run_plan p;
     rc = resolve_plan(g, tuning, &p);
     if (rc) return rc;
-    if (plan) *plan = cb2_tuning{p.k, p.tile_rows, p.v, p.l};
+    if (plan) *plan = cb2_tuning{p.k, p.tile_rows, p.v, p.l, p.r};
     return CB2_OK;
+}
+
+int cb2_variants(int automaton, cb2_tuning* out, int capacity) {
+    if (planes_of(automaton) < 0) return fail(CB2_ENOTFOUND, "unknown automaton id " + std::to_string(automaton));
+    const std::vector<strip_variant>& vs = strip_variants(automaton);
+    for (int i = 0; out && i < capacity && i < (int)vs.size(); ++i)
+        out[i] = cb2_tuning{vs[i].k, 0, vs[i].v, vs[i].l, vs[i].r};
+    return (int)vs.size();
 }
 
 int cb2_autotune(int automaton, int64_t x_size, int64_t y_size, double budget_ms, cb2_tuning* best) {
@@ -448,8 +468,8 @@ int cb2_autotune(int automaton, int64_t x_size, int64_t y_size, double budget_ms
     for (const strip_variant& sv : strip_variants(automaton)) {
         if (sv.k < 4) continue;  // one- and two-generation passes are memory-bound at any size
         const int rows = auto_tile_rows(g, sv);
-        cands.push_back(cb2_tuning{sv.k, rows, sv.v, sv.l});
-        if (rows * 2 <= (int)g.h) cands.push_back(cb2_tuning{sv.k, rows * 2, sv.v, sv.l});
+        cands.push_back(cb2_tuning{sv.k, rows, sv.v, sv.l, sv.r});
+        if (rows * 2 <= (int)g.h) cands.push_back(cb2_tuning{sv.k, rows * 2, sv.v, sv.l, sv.r});
     }
     double best_ns = 1e300;
     cb2_tuning pick = cands.front();
@@ -498,9 +518,11 @@ int cb2_tuning_load(const char* path) {
         cb2_tuning t{};
         if (!(is >> name >> x >> y >> t.temporal_steps >> t.tile_rows >> t.words_per_lane >> t.levels_per_warp))
             return fail(CB2_EINVAL, "malformed tuning line: " + line);
+        if (!(is >> t.rows_per_step)) t.rows_per_step = 1;  // lines written before the field existed
         int a = find_automaton(name.c_str());
         if (a < 0) return fail(CB2_ENOTFOUND, "unknown automaton in tuning file: " + name);
-        if (!valid_k(t.temporal_steps) || !find_variant(a, t.temporal_steps, t.words_per_lane, t.levels_per_warp) ||
+        if (!valid_k(t.temporal_steps) ||
+            !find_variant(a, t.temporal_steps, t.words_per_lane, t.levels_per_warp, t.rows_per_step) ||
             t.tile_rows < 1)
             return fail(CB2_EINVAL, "invalid tuning values: " + line);
         std::lock_guard<std::mutex> lock(g_tune_mu);
@@ -513,12 +535,12 @@ int cb2_tuning_load(const char* path) {
 int cb2_tuning_save(const char* path) {
     std::ofstream f(path ? path : "");
     if (!f) return fail(CB2_EINVAL, std::string("cannot write tuning file ") + (path ? path : "(null)"));
-    f << "# automaton x_size y_size temporal_steps tile_rows words_per_lane levels_per_warp\n";
+    f << "# automaton x_size y_size temporal_steps tile_rows words_per_lane levels_per_warp rows_per_step\n";
     std::lock_guard<std::mutex> lock(g_tune_mu);
     for (auto& kv : g_tune)
         f << kNames[kv.first.automaton] << ' ' << kv.first.x << ' ' << kv.first.y << ' ' << kv.second.temporal_steps
           << ' ' << kv.second.tile_rows << ' ' << kv.second.words_per_lane << ' ' << kv.second.levels_per_warp
-          << '\n';
+          << ' ' << kv.second.rows_per_step << '\n';
     return (int)g_tune.size();
 }
 

@@ -59,7 +59,7 @@ int cb2_band_pass(int automaton, void* const* in, void* const* out, int64_t x_si
         set_error("a pass of " + std::to_string(temporal_steps) + " generations needs that many ghost rows each side");
         return CB2_EINVAL;
     }
-    cb2_tuning t{temporal_steps, 0, 0, 0};
+    cb2_tuning t{temporal_steps, 0, 0, 0, 0};
     if (tuning) {
         t = *tuning;
         t.temporal_steps = temporal_steps;

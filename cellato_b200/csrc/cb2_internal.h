@@ -26,15 +26,16 @@ struct grid_geom {
 
 // Tuning knobs for one single-grid run.
 struct run_plan {
-    int k;          // generations per launch (1, 2, 4, 8 or 16)
+    int k;          // generations per launch (1, 2, 4, 8, 16 or 32)
     int v;          // 32-bit words per lane (1, 2 or 4)
     int l;          // levels (generations) per warp; the CTA has k / l warps
+    int r;          // rows each warp takes per barrier (1, 2 or 4)
     int tile_rows;  // output rows per strip task
 };
 
 // One instantiated strip kernel.
 struct strip_variant {
-    int k, v, l;
+    int k, v, l, r;
     const void* fn;
     int threads;
     int smem_bytes;
@@ -53,9 +54,9 @@ cudaError_t launch_strip_window(const grid_geom& g, const uint32_t* in, uint32_t
 // Strip tasks per column and per row for a plan.
 void strip_counts(const grid_geom& g, int v, int tile_rows, int* nsx, int* nsy);
 // The instantiated kernels of an automaton, and the first one matching a
-// plan (v or l of 0 match anything).
+// plan (v, l or r of 0 match anything).
 const std::vector<strip_variant>& strip_variants(int automaton);
-const strip_variant* find_variant(int automaton, int k, int v, int l);
+const strip_variant* find_variant(int automaton, int k, int v, int l, int r = 0);
 // Output rows per task so that one launch fills the GPU about once.
 int auto_tile_rows(const grid_geom& g, const strip_variant& sv);
 // Number of strip-task CTAs resident at once on this device.

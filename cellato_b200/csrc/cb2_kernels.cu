@@ -1,7 +1,7 @@
 // cb2_kernels.cu -- device kernels of the library and their launchers.
 //
-//  * pipe_kernel<Rule, K, V, L> the hot path (cb2_pipe.cuh), K generations
-//                               per launch over a whole grid
+//  * pipe_kernel<Rule, K, V, L, RPS> the hot path (cb2_pipe.cuh), K
+//                               generations per launch over a whole grid
 //  * layout conversion kernels  standard / bit_array / tiled host images to
 //                               and from the device's linear bit planes
 //  * fill_random_kernel         the seeded SplitMix64 input generator
@@ -34,7 +34,7 @@ struct strip_launch {
     int32_t y_base, rows_out;  // output rows [y_base, y_base + rows_out)
 };
 
-template <class R, int K, int V, int L>
+template <class R, int K, int V, int L, int RPS>
 __global__ void __launch_bounds__(32 * (K / L)) pipe_kernel(strip_launch a) {
     extern __shared__ __align__(16) uint32_t smem[];
     constexpr int own = 32 * V - 2;
@@ -50,20 +50,25 @@ __global__ void __launch_bounds__(32 * (K / L)) pipe_kernel(strip_launch a) {
     t.nx = min(own, a.wd - t.x0);
     t.y0 = a.y_base + sy * a.tile_rows;
     t.ny = min(a.tile_rows, a.y_base + a.rows_out - t.y0);
-    if constexpr (L == K)
+    if constexpr (RPS > 1)
+        pipe_run_rows<R, K, V, L, kRingDepth, RPS>(t, smem);  // RPS rows per barrier
+    else if constexpr (L == K)
         warp_run<R, K, V, kRingDepth>(t, strip_geom<V>(t, threadIdx.x & 31), smem);  // one warp, skewed levels
     else
         pipe_run<R, K, V, L, kRingDepth>(t, smem);
 }
 
-template <class R, int K, int V, int L>
+template <class R, int K, int V, int L, int RPS = 1>
 static strip_variant make_variant() {
-    const int words = L == K ? warp_smem_words<R, V, kRingDepth>() : pipe_smem_words<R, K, V, L, kRingDepth>();
-    return strip_variant{K, V, L, (const void*)pipe_kernel<R, K, V, L>, 32 * (K / L), 4 * words};
+    const int words = RPS > 1  ? pipe_rows_smem_words<R, K, V, L, kRingDepth, RPS>()
+                      : L == K ? warp_smem_words<R, V, kRingDepth>()
+                               : pipe_smem_words<R, K, V, L, kRingDepth>();
+    return strip_variant{K, V, L, RPS, (const void*)pipe_kernel<R, K, V, L, RPS>, 32 * (K / L), 4 * words};
 }
 
-// The instantiated (K, V, L) plans; for each (K, V) the first entry is the
-// default levels-per-warp.
+// The instantiated (K, V, L, rows per step) plans; for each (K, V) the first
+// entry is the default levels-per-warp, for each (K, V, L) the first entry
+// the default rows per step.
 template <class R>
 static const std::vector<strip_variant>& variants_for() {
     static const std::vector<strip_variant> v = {
@@ -75,6 +80,10 @@ static const std::vector<strip_variant>& variants_for() {
         make_variant<R, 16, 2, 2>(), make_variant<R, 16, 2, 4>(), make_variant<R, 16, 4, 2>(),
         make_variant<R, 16, 1, 4>(), make_variant<R, 8, 2, 8>(),  make_variant<R, 16, 1, 16>(),
         make_variant<R, 4, 4, 4>(),
+        make_variant<R, 16, 2, 8, 4>(), make_variant<R, 16, 2, 8, 2>(), make_variant<R, 16, 2, 4, 4>(),
+        make_variant<R, 16, 2, 16, 4>(), make_variant<R, 16, 1, 16, 4>(),
+        make_variant<R, 32, 2, 16, 4>(), make_variant<R, 32, 2, 8, 4>(), make_variant<R, 32, 2, 8, 2>(),
+        make_variant<R, 32, 2, 4, 4>(), make_variant<R, 32, 1, 16, 4>(), make_variant<R, 32, 1, 32, 4>(),
     };
     return v;
 }
@@ -89,9 +98,9 @@ const std::vector<strip_variant>& strip_variants(int automaton) {
     }
 }
 
-const strip_variant* find_variant(int automaton, int k, int v, int l) {
+const strip_variant* find_variant(int automaton, int k, int v, int l, int r) {
     for (const strip_variant& sv : strip_variants(automaton))
-        if (sv.k == k && (v == 0 || sv.v == v) && (l == 0 || sv.l == l)) return &sv;
+        if (sv.k == k && (v == 0 || sv.v == v) && (l == 0 || sv.l == l) && (r == 0 || sv.r == r)) return &sv;
     return nullptr;
 }
 
@@ -149,7 +158,7 @@ int auto_tile_rows(const grid_geom& g, const strip_variant& sv) {
 
 cudaError_t launch_strip_window(const grid_geom& g, const uint32_t* in, uint32_t* out, const run_plan& plan,
                                 int y_base, int rows_out, cudaStream_t stream) {
-    const strip_variant* sv = find_variant(g.automaton, plan.k, plan.v, plan.l);
+    const strip_variant* sv = find_variant(g.automaton, plan.k, plan.v, plan.l, plan.r);
     if (!sv || rows_out < 1 || y_base < 0 || y_base + rows_out > g.h) return cudaErrorInvalidValue;
     resident_strip_tasks(*sv);  // sets the kernel's shared-memory attribute once
     strip_launch a;

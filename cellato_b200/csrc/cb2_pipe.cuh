@@ -15,7 +15,8 @@
 //   warp W-1    writes the finished row (generation t+K) to global memory
 //
 // One __syncthreads per step separates the slot a warp writes from the slot
-// its successor reads.  The row bookkeeping is the single-warp wavefront's:
+// its successor reads.  pipe_run_rows is the same pipeline with RPS rows per
+// step (RPS-row slots, one barrier per RPS rows).  The row bookkeeping is the single-warp wavefront's:
 // input row r (sweep coordinates) leaves warp W-1 at step r + W - 1 as output
 // row r - K, so rows before the 2K-row warm-up are computed but never stored.
 #pragma once
@@ -89,6 +90,7 @@ __device__ __forceinline__ void slot_write(uint32_t* slot, int lane, const uint3
 template <class R, int K, int V, int L, int DEPTH>
 __device__ __forceinline__ void pipe_run(const strip_task& t, uint32_t* smem) {
     static_assert(K % L == 0, "levels per warp must divide K");
+    static_assert(K <= 32, "the one-word halo of a strip covers at most 32 generations");
     static_assert(DEPTH >= 2, "input ring of at least two rows");
     constexpr int W = K / L;
     constexpr int P = R::P;
@@ -168,6 +170,120 @@ __device__ __forceinline__ void pipe_run(const strip_task& t, uint32_t* smem) {
     for (int st = 0; st < steps; st += 2) {
         step(st, std::integral_constant<int, 0>{});
         if (st + 1 < steps) step(st + 1, std::integral_constant<int, 1>{});
+    }
+    if (warp == 0) cp_async_wait<0>();
+}
+
+// Shared memory of pipe_run_rows in 32-bit words: the input ring plus two
+// RPS-row hand-off slots per warp boundary.
+template <class R, int K, int V, int L, int DEPTH, int RPS>
+constexpr int pipe_rows_smem_words() {
+    return (DEPTH + 2 * RPS * (K / L - 1)) * R::P * 32 * V;
+}
+
+// pipe_run with RPS (even) rows per step: every warp pushes RPS consecutive
+// rows through its levels between two barriers, which divides the barriers
+// and the per-step bookkeeping per row by RPS.  Row j of a step uses level
+// slot j & 1, so no step parity is needed.  cp.async groups hold RPS rows;
+// the ring of DEPTH rows keeps DEPTH / RPS - 1 groups in flight.
+template <class R, int K, int V, int L, int DEPTH, int RPS>
+__device__ __forceinline__ void pipe_run_rows(const strip_task& t, uint32_t* smem) {
+    static_assert(K % L == 0, "levels per warp must divide K");
+    static_assert(K <= 32, "the one-word halo of a strip covers at most 32 generations");
+    static_assert(RPS >= 2 && RPS % 2 == 0, "an even number of rows per step");
+    static_assert(DEPTH % RPS == 0 && DEPTH / RPS >= 2, "a ring of at least two groups of rows");
+    constexpr int W = K / L;
+    constexpr int P = R::P;
+    constexpr int SLOT = P * 32 * V;  // words per row
+    constexpr int G = DEPTH / RPS;    // groups of RPS rows in the ring
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const lane_geom<V> geom = strip_geom<V>(t, lane);
+
+    strip_state<R, L, V> s;
+#pragma unroll
+    for (int g = 0; g < L; ++g)
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int i = 0; i < V; ++i) {
+#pragma unroll
+                for (int k = 0; k < R::NH; ++k) s.h[g][q][i][k] = 0;
+#pragma unroll
+                for (int p = 0; p < P; ++p) s.c[g][q][i][p] = 0;
+            }
+
+    uint32_t* ring = smem;
+    uint32_t* hand = smem + DEPTH * SLOT;  // boundary b, parity q: hand + (2b + q) * RPS * SLOT
+    const int total = t.ny + 2 * K;
+    const int steps = (total + RPS - 1) / RPS + W - 1;
+
+    int lr = 0;
+    auto issue = [&](int g) {  // rows [g*RPS, (g+1)*RPS) as one group
+#pragma unroll
+        for (int j = 0; j < RPS; ++j) {
+            const int r = g * RPS + j;
+            if (r < total) {
+                const uint32_t* base = t.in + (int64_t)lr * t.wd;
+                uint32_t* dst = ring + (r % DEPTH) * SLOT;
+#pragma unroll
+                for (int p = 0; p < P; ++p)
+#pragma unroll
+                    for (int i = 0; i < V; ++i)
+                        cp_async4(dst + (p * 32 + lane) * V + i, base + p * t.plane_words + geom.col[i]);
+                lr = lr + 1 == t.h ? 0 : lr + 1;
+            }
+        }
+        cp_async_commit();
+    };
+    if (warp == 0) {
+        lr = (t.y0 - K) % t.h;
+        if (lr < 0) lr += t.h;
+#pragma unroll
+        for (int g = 0; g < G - 1; ++g) issue(g);
+    } else {
+        for (int j = lane; j < 2 * RPS * SLOT; j += 32) hand[(warp - 1) * 2 * RPS * SLOT + j] = 0;
+    }
+    __syncthreads();
+
+    for (int st = 0; st < steps; ++st) {
+        uint32_t rows[RPS][V][P];
+        if (warp == 0) {
+            issue(st + G - 1);
+            cp_async_wait<G - 1>();
+#pragma unroll
+            for (int j = 0; j < RPS; ++j) {
+                const int r = RPS * st + j;
+                if (r < total) {
+                    slot_read<R, V>(ring + (r % DEPTH) * SLOT, lane, rows[j]);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < V; ++i)
+#pragma unroll
+                        for (int p = 0; p < P; ++p) rows[j][i][p] = 0;
+                }
+            }
+        } else {
+            const uint32_t* in = hand + ((warp - 1) * 2 + (st & 1)) * RPS * SLOT;
+#pragma unroll
+            for (int j = 0; j < RPS; ++j) slot_read<R, V>(in + j * SLOT, lane, rows[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < RPS; j += 2) {
+            strip_push<R, L, V, 0>(s, rows[j], geom.src_l, geom.src_r);
+            strip_push<R, L, V, 1>(s, rows[j + 1], geom.src_l, geom.src_r);
+        }
+        if (warp == W - 1) {
+            const int r0 = RPS * (st - (W - 1));  // input rows whose results leave now
+#pragma unroll
+            for (int j = 0; j < RPS; ++j)
+                if (r0 + j >= 2 * K && r0 + j < total) strip_store<R, V>(t, geom, r0 + j - 2 * K, rows[j]);
+        } else {
+            uint32_t* out = hand + (warp * 2 + ((st + 1) & 1)) * RPS * SLOT;
+#pragma unroll
+            for (int j = 0; j < RPS; ++j) slot_write<R, V>(out + j * SLOT, lane, rows[j]);
+        }
+        __syncthreads();
     }
     if (warp == 0) cp_async_wait<0>();
 }

@@ -254,7 +254,7 @@ bool server_impl::admit_locked(std::vector<request_state*>& newly) {
 void server_impl::run_one(request_state* r) {
     uint32_t* const bufs[2] = {r->grid.buf[0], r->grid.buf[1]};
     int res = 0;
-    cb2_tuning t{opts.temporal_steps, 0, 0, 0};
+    cb2_tuning t{opts.temporal_steps, 0, 0, 0, 0};
     int rc = run_chunks(r->grid.g, bufs, 0, r->req.steps, &t, stream, &res);
     if (rc) {
         finish(r, rc, cb2_last_error());

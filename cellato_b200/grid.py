@@ -185,8 +185,8 @@ class DeviceGrid:
 
     # the hot path -----------------------------------------------------------------------------
     def run(self, steps: int, temporal_steps: int = 0, tile_rows: int = 0, words_per_lane: int = 0,
-            levels_per_warp: int = 0, stream=None) -> None:
-        t = _abi.tuning(temporal_steps, tile_rows, words_per_lane, levels_per_warp)
+            levels_per_warp: int = 0, stream=None, rows_per_step: int = 0) -> None:
+        t = _abi.tuning(temporal_steps, tile_rows, words_per_lane, levels_per_warp, rows_per_step)
         check(lib.cb2_grid_run(self._h, steps, ctypes.byref(t), _stream_handle(stream)), "run")
 
     def checksum(self, values=None, stream=None) -> list[int]:
@@ -269,9 +269,9 @@ class Batch:
 
 
 def plan(automaton, x_size: int, y_size: int, temporal_steps: int = 0, tile_rows: int = 0,
-         words_per_lane: int = 0, levels_per_warp: int = 0) -> dict:
-    """The plan (temporal depth, strip height, lane width, levels per warp) a run would use."""
-    want = _abi.tuning(temporal_steps, tile_rows, words_per_lane, levels_per_warp)
+         words_per_lane: int = 0, levels_per_warp: int = 0, rows_per_step: int = 0) -> dict:
+    """The plan (temporal depth, strip height, lane width, levels per warp, rows per step) a run would use."""
+    want = _abi.tuning(temporal_steps, tile_rows, words_per_lane, levels_per_warp, rows_per_step)
     got = _abi.Tuning()
     check(lib.cb2_plan(automaton_id(automaton), x_size, y_size, ctypes.byref(want), ctypes.byref(got)), "plan")
     return got.as_dict()
@@ -279,15 +279,24 @@ def plan(automaton, x_size: int, y_size: int, temporal_steps: int = 0, tile_rows
 
 def run_bit_planes(automaton, a_planes: list[int], b_planes: list[int], x_size: int, y_size: int, steps: int,
                    temporal_steps: int = 0, tile_rows: int = 0, words_per_lane: int = 0, levels_per_warp: int = 0,
-                   stream=None) -> bool:
+                   stream=None, rows_per_step: int = 0) -> bool:
     """Advances caller-owned device planes; returns True if the result is in ``b_planes``."""
     a = (ctypes.c_void_p * len(a_planes))(*a_planes)
     b = (ctypes.c_void_p * len(b_planes))(*b_planes)
-    t = _abi.tuning(temporal_steps, tile_rows, words_per_lane, levels_per_warp)
+    t = _abi.tuning(temporal_steps, tile_rows, words_per_lane, levels_per_warp, rows_per_step)
     res = ctypes.c_int()
     check(lib.cb2_run_bit_planes(automaton_id(automaton), a, b, x_size, y_size, steps, ctypes.byref(t),
                                  _stream_handle(stream), ctypes.byref(res)), "run_bit_planes")
     return bool(res.value)
+
+
+def variants(automaton) -> list[tuple[int, int, int, int]]:
+    """The instantiated strip kernels as (temporal_steps, words_per_lane, levels_per_warp, rows_per_step)."""
+    a = automaton_id(automaton)
+    n = check(lib.cb2_variants(a, None, 0), "variants")
+    arr = (_abi.Tuning * n)()
+    check(lib.cb2_variants(a, arr, n), "variants")
+    return [(t.temporal_steps, t.words_per_lane, t.levels_per_warp, t.rows_per_step) for t in arr]
 
 
 def autotune(automaton, x_size: int, y_size: int, budget_ms: float = 0.0) -> dict:

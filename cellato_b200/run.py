@@ -38,6 +38,7 @@ def parse(argv):
     ap.add_argument("--temporal_tile_size_y", type=int, default=0)
     ap.add_argument("--words_per_lane", type=int, default=0)
     ap.add_argument("--levels_per_warp", type=int, default=0)
+    ap.add_argument("--rows_per_step", type=int, default=0)
     ap.add_argument("--rounds", type=int, default=1)
     ap.add_argument("--warmup_rounds", type=int, default=0)
     ap.add_argument("--seed", type=int, default=42)
@@ -63,8 +64,8 @@ def validate(a) -> None:
         raise ValueError(f"Invalid --x_size {a.x_size}: must be divisible by 32")
     if a.steps < 0:
         raise ValueError(f"Invalid --steps {a.steps}")
-    if a.temporal_steps not in (0, 1, 2, 4, 8, 16):
-        raise ValueError(f"Invalid --temporal_steps {a.temporal_steps}: use 1, 2, 4, 8 or 16")
+    if a.temporal_steps not in (0, 1, 2, 4, 8, 16, 32):
+        raise ValueError(f"Invalid --temporal_steps {a.temporal_steps}: use 1, 2, 4, 8, 16 or 32")
     if a.layout != "standard":
         G.layout_bytes(a.automaton, a.layout, a.word_size, a.x_size, a.y_size)
 
@@ -93,7 +94,7 @@ def main(argv=None) -> int:
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             g.run(a.steps, a.temporal_steps, a.temporal_tile_size_y, a.words_per_lane, a.levels_per_warp,
-                  stream=stream)
+                  stream=stream, rows_per_step=a.rows_per_step)
             e1.record(stream)
             e1.synchronize()
             if r >= a.warmup_rounds:

@@ -46,6 +46,7 @@ class RunParams:
     cuda_block_size_y: int = 8
     words_per_lane: int = 0
     levels_per_warp: int = 0
+    rows_per_step: int = 0
 
     def csv_line(self) -> str:
         f = self
@@ -74,8 +75,8 @@ class Traverser:
         self._params = RunParams()
 
     def init(self, grid: HostGrid, params: RunParams) -> None:
-        if params.temporal_steps not in (0, 1, 2, 4, 8, 16):
-            raise ValueError(f"Invalid --temporal_steps {params.temporal_steps}: use 1, 2, 4, 8 or 16")
+        if params.temporal_steps not in (0, 1, 2, 4, 8, 16, 32):
+            raise ValueError(f"Invalid --temporal_steps {params.temporal_steps}: use 1, 2, 4, 8, 16 or 32")
         self._params = params
         self._layout, self._word_bits = grid.layout, grid.word_bits
         self._grid = DeviceGrid(grid.automaton, grid.x_size, grid.y_size)
@@ -87,7 +88,7 @@ class Traverser:
         p = self._params
         if callback is None:
             self._grid.run(steps, p.temporal_steps, p.temporal_tile_size_y, p.words_per_lane, p.levels_per_warp,
-                           stream=stream)
+                           stream=stream, rows_per_step=p.rows_per_step)
             return
         # Callback after every chunk with the host grid, like temporal.cuh:230-232.
         chunk = p.temporal_steps or 1
@@ -95,8 +96,9 @@ class Traverser:
         done = 0
         while done < steps:
             n = min(chunk, steps - done)
-            self._grid.run(n, n if n in (1, 2, 4, 8, 16) else 0, p.temporal_tile_size_y, p.words_per_lane,
-                           p.levels_per_warp if n == chunk else 0, stream=stream)
+            self._grid.run(n, n if n in (1, 2, 4, 8, 16, 32) else 0, p.temporal_tile_size_y, p.words_per_lane,
+                           p.levels_per_warp if n == chunk else 0, stream=stream,
+                           rows_per_step=p.rows_per_step if n == chunk else 0)
             done += n
             callback(done, self._grid.download(self._layout, self._word_bits, stream))
 

@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define CB2_ABI_VERSION 1
+#define CB2_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------- */
 #define CB2_OK 0
@@ -75,11 +75,14 @@ int cb2_automaton_info(int id, const char** name, int* planes, int* states);
  * Replaces --temporal_steps / --temporal_tile_size_y / --cuda_block_size_*
  * (experiments/run_params.hpp:10-43). */
 typedef struct cb2_tuning {
-    int temporal_steps;  /* generations per HBM round trip: 1, 2, 4, 8, 16  */
+    int temporal_steps;  /* generations per HBM round trip: 1, 2, 4, 8, 16,
+                            32                                              */
     int tile_rows;       /* output rows per strip task (one CTA)            */
     int words_per_lane;  /* 32-bit words per lane: 1, 2 or 4                */
     int levels_per_warp; /* generations each warp of the CTA holds; the CTA
                             has temporal_steps / levels_per_warp warps      */
+    int rows_per_step;   /* rows each warp passes on between two CTA
+                            barriers: 1, 2 or 4                             */
 } cb2_tuning;
 
 /* ---- caller-owned device planes ----------------------------------------- */
@@ -285,12 +288,19 @@ int cb2_server_destroy(cb2_server* server);
  * cb2_tuning field is 0) and returns it in *best.  `budget_ms` bounds the
  * time spent (<= 0: a default). */
 int cb2_autotune(int automaton, int64_t x_size, int64_t y_size, double budget_ms, cb2_tuning* best);
-/* Loads / saves the tuning table as text lines
- * "automaton x_size y_size temporal_steps tile_rows words_per_lane levels_per_warp". */
+/* Loads / saves the tuning table as text lines "automaton x_size y_size
+ * temporal_steps tile_rows words_per_lane levels_per_warp rows_per_step"
+ * (lines without the last field load with rows_per_step 1). */
 int cb2_tuning_load(const char* path);
 int cb2_tuning_save(const char* path);
 /* The plan cb2_grid_run would use for a chunk of `steps` generations. */
 int cb2_plan(int automaton, int64_t x_size, int64_t y_size, const cb2_tuning* tuning, cb2_tuning* plan);
+/* The strip kernels instantiated for `automaton`: writes up to `capacity`
+ * of them to out[] (temporal_steps, words_per_lane, levels_per_warp,
+ * rows_per_step set; tile_rows 0) and returns how many there are.  The
+ * reference's temporal traverser has one kernel shape; the table is what
+ * cb2_autotune chooses from. */
+int cb2_variants(int automaton, cb2_tuning* out, int capacity);
 
 /* Measured peak of 32-bit three-input logic ops on the current device
  * (ops/s), the integer roof of the rule networks. */

@@ -179,8 +179,8 @@ public:
         _x = layout::x(grid);
         _y = layout::y(grid);
         const int k = params.temporal_steps;
-        _tuning = cb2_tuning{(k == 1 || k == 2 || k == 4 || k == 8 || k == 16) ? k : 0,
-                             params.temporal_tile_size_y > 0 ? params.temporal_tile_size_y : 0, 0, 0};
+        _tuning = cb2_tuning{(k == 1 || k == 2 || k == 4 || k == 8 || k == 16 || k == 32) ? k : 0,
+                             params.temporal_tile_size_y > 0 ? params.temporal_tile_size_y : 0, 0, 0, 0};
         cb2_grid* g = nullptr;
         check(cb2_grid_create(id, _x, _y, &g), "cb2_grid_create");
         _grid.reset(g);

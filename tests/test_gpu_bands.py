@@ -33,7 +33,7 @@ def test_single_rank_band_equals_grid(cuda, a):
     assert (b.band_planes_host().numpy() == planes).all()
 
 
-@pytest.mark.parametrize("a,k", [(0, 16), (1, 8), (2, 4)])
+@pytest.mark.parametrize("a,k", [(0, 16), (1, 8), (2, 4), (0, 32), (2, 32)])
 def test_two_bands_on_one_gpu_equal_the_global_grid(cuda, a, k):
     torch = cuda
     x, rows, steps = 4096, 96, 45

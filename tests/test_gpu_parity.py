@@ -18,11 +18,15 @@ PLANS = [dict(), dict(temporal_steps=1), dict(temporal_steps=2, words_per_lane=1
          dict(temporal_steps=8, words_per_lane=1, tile_rows=64), dict(temporal_steps=8, words_per_lane=4),
          dict(temporal_steps=16, words_per_lane=2, levels_per_warp=2),
          dict(temporal_steps=16, words_per_lane=1, levels_per_warp=4, tile_rows=3),
-         dict(temporal_steps=8, words_per_lane=2, levels_per_warp=2)]
-# every instantiated (K, V, L)
-VARIANTS = [(1, 2, 1), (1, 1, 1), (1, 4, 1), (2, 2, 2), (2, 2, 1), (2, 1, 2), (4, 2, 4), (4, 2, 2), (4, 1, 4),
-            (4, 4, 2), (8, 2, 4), (8, 2, 2), (8, 1, 8), (8, 1, 4), (8, 4, 2), (16, 2, 2), (16, 2, 4), (16, 4, 2),
-            (16, 1, 4), (8, 2, 8), (16, 1, 16), (4, 4, 4)]
+         dict(temporal_steps=8, words_per_lane=2, levels_per_warp=2),
+         dict(temporal_steps=32), dict(temporal_steps=32, words_per_lane=2, levels_per_warp=4, rows_per_step=4,
+                                       tile_rows=7),
+         dict(temporal_steps=16, words_per_lane=2, levels_per_warp=8, rows_per_step=2, tile_rows=1)]
+
+
+def variants(a):
+    """Every instantiated (K, V, L, rows per step) of automaton a."""
+    return cb.variants(a)
 
 
 def device_run(automaton, cells, steps, **plan):
@@ -65,8 +69,8 @@ def test_random_shapes_and_plans(cuda):
         x = 32 * rng.choice([1, 2, 3, 5, 29, 30, 31, 32, 61, 62, 63, 64, 65, 97])
         y = rng.choice([1, 2, 3, 7, 16, 17, 64, 101])
         steps = rng.randrange(0, 40)
-        k, v, lv = rng.choice(VARIANTS)
-        plan = dict(temporal_steps=k, words_per_lane=v, levels_per_warp=lv,
+        k, v, lv, r = rng.choice(variants(a))
+        plan = dict(temporal_steps=k, words_per_lane=v, levels_per_warp=lv, rows_per_step=r,
                     tile_rows=rng.choice([0, 1, 2, 3, 9, 1000]))
         cells = O.init_cells(x, y, trial, O.thresholds(PROBS[a]))
         got, ck = device_run(a, cells, steps, **plan)
@@ -146,10 +150,10 @@ def test_every_variant_on_a_ragged_grid(cuda):
     for a in (0, 1, 2):
         cells = O.init_cells(x, y, 1234 + a, O.thresholds(PROBS[a]))
         want = O.run_standard(a, cells, steps)
-        for (k, v, lv) in VARIANTS:
+        for (k, v, lv, r) in variants(a):
             got, _ = device_run(a, cells, steps, temporal_steps=k, words_per_lane=v, levels_per_warp=lv,
-                                tile_rows=11)
-            assert (got == want).all(), (a, k, v, lv)
+                                rows_per_step=r, tile_rows=11)
+            assert (got == want).all(), (a, k, v, lv, r)
 
 
 def test_plan_resolution(cuda):
@@ -160,6 +164,16 @@ def test_plan_resolution(cuda):
         cb.plan("game-of-life", 4096, 4096, temporal_steps=2, words_per_lane=4, levels_per_warp=2)
     with pytest.raises(ValueError, match="temporal_steps must be"):
         cb.plan("wire", 4096, 4096, temporal_steps=3)
+    with pytest.raises(ValueError, match="rows_per_step must be"):
+        cb.plan("wire", 4096, 4096, temporal_steps=16, rows_per_step=3)
+    with pytest.raises(ValueError, match="no strip kernel"):
+        cb.plan("wire", 4096, 4096, temporal_steps=16, words_per_lane=2, levels_per_warp=2, rows_per_step=4)
+    p = cb.plan("excitable", 32768, 32768, temporal_steps=32, words_per_lane=2, levels_per_warp=8, rows_per_step=4)
+    assert (p["temporal_steps"], p["levels_per_warp"], p["rows_per_step"]) == (32, 8, 4)
+    for a in (0, 1, 2):  # every variant resolves to itself
+        for (k, v, lv, r) in variants(a):
+            p = cb.plan(a, 8192, 8192, temporal_steps=k, words_per_lane=v, levels_per_warp=lv, rows_per_step=r)
+            assert (p["temporal_steps"], p["words_per_lane"], p["levels_per_warp"], p["rows_per_step"]) == (k, v, lv, r)
 
 
 def test_caller_owned_planes(cuda):
