@@ -325,6 +325,9 @@ def main() -> None:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="gol-65536", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="run the library's default plan instead of timing candidates first (for profiler runs, "
+                         "whose serialised launches distort the candidates' timings)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
@@ -352,7 +355,7 @@ def main() -> None:
     name, P, _ = cb.automaton_info(a)
     cells = x * y
     stream = torch.cuda.current_stream()
-    tuned = cb.autotune(a, x, y, budget_ms=4000)
+    tuned = None if args.no_autotune else cb.autotune(a, x, y, budget_ms=4000)
     plan = cb.plan(a, x, y)
     k = plan["temporal_steps"]
     if world == 1:
@@ -362,10 +365,14 @@ def main() -> None:
         # one grid of world*y rows split into bands, one per rank (NCCL halo exchange per pass)
         from cellato_b200.bands import BandGrid
 
-        cb.autotune(a, x, y, budget_ms=4000)
         grid = BandGrid(a, x, y * world, rank, world)
         grid.fill_random(wl["seed"], wl["probs"], stream=stream)
-        k = grid.plan_k()
+        # every rank must take the same passes (one halo exchange each): use rank 0's depth
+        kt = torch.tensor([grid.plan_k()], dtype=torch.int64, device="cuda")
+        dist.broadcast(kt, 0)
+        k = int(kt.item())
+
+    run_kw = {} if world == 1 else {"temporal_steps": k}
 
     def barrier():
         if world > 1:
@@ -380,7 +387,7 @@ def main() -> None:
 
     # ---- device-resident timing ----
     for _ in range(args.warmup):
-        grid.run(gens, stream=stream)
+        grid.run(gens, **run_kw, stream=stream)
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
@@ -388,7 +395,7 @@ def main() -> None:
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        grid.run(gens, stream=stream)
+        grid.run(gens, **run_kw, stream=stream)
     e1.record(stream)
     e1.synchronize()
     torch.cuda.synchronize()
@@ -443,7 +450,7 @@ def main() -> None:
 
         def e2e_step():
             grid.upload(host_img, stream=stream)
-            grid.run(gens, stream=stream)
+            grid.run(gens, **run_kw, stream=stream)
             grid.download("bit_planes", 64, stream=stream, out=host_out.numpy())
     else:
         g0, nb = grid.ghost, grid.band
@@ -453,7 +460,7 @@ def main() -> None:
 
         def e2e_step():
             grid.planes[:, g0:g0 + nb].copy_(band_in, non_blocking=True)
-            grid.run(gens, stream=stream)
+            grid.run(gens, **run_kw, stream=stream)
             band_out.copy_(grid.planes[:, g0:g0 + nb], non_blocking=True)
             torch.cuda.current_stream().synchronize()
     e2e_step()
@@ -499,7 +506,8 @@ def main() -> None:
         "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": wl["desc"], "automaton": name, "x_size": x, "y_size": y,
                    "generations_per_step": gens, "plan": plan, "autotuned": tuned,
-                   "l2": "inputs larger than L2 (each plane buffer is 512 MiB at 65536^2)",
+                   "l2": (f"inputs larger than L2: each of the {P} plane(s) of each buffer is "
+                          f"{x * y // 8 // 2**20} MiB at {x}x{y}; a K-generation pass streams all of them"),
                    "parallelism": (f"row bands x{world}: one {x}x{y * world} grid, {y} rows per GPU, NCCL halo "
                                    f"exchange of K rows each way per pass" if world > 1 else "single GPU")},
         "roofline": roof,
