@@ -262,13 +262,13 @@ def serve_workload(n: int, seed: int = 7):
     return out
 
 
-def serve_stream(cb, specs, rate: float, per_request: bool, seed: int = 11) -> dict:
+def serve_stream(cb, specs, rate: float, per_request: bool, seed: int = 11, **server_opts) -> dict:
     """Submits `specs` with Poisson arrivals at `rate` req/s; returns latency
     percentiles (submit to result) and throughput over the makespan."""
     import numpy as np
 
     gaps = np.random.default_rng(seed).exponential(1.0 / rate, len(specs))
-    with cb.Server(per_request=per_request) as srv:
+    with cb.Server(per_request=per_request, **server_opts) as srv:
         t0 = time.perf_counter()
         due = 0.0
         ids = []
@@ -279,12 +279,14 @@ def serve_stream(cb, specs, rate: float, per_request: bool, seed: int = 11) -> d
             ids.append(srv.submit(a, x, y, steps, sd, BATCH_PROBS[a]))
         srv.drain(1200)
         st = [srv.status(i) for i in ids]
+        stats = srv.stats()
     lat = np.array([r["done_s"] - r["submit_s"] for r in st])
     span = max(r["done_s"] for r in st) - min(r["submit_s"] for r in st)
     cells = sum(x * y * steps for (_, x, y, steps, _) in specs)
     return {"rate_req_s": rate, "requests": len(specs), "failed": sum(r["state"] != "done" for r in st),
             "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
-            "throughput": cells / span / 1e9, "makespan_s": span}
+            "throughput": cells / span / 1e9, "makespan_s": span, "rounds": stats["rounds"],
+            "server_plan_s": stats["plan_s"], "server_wait_s": stats["wait_s"], "batch_tasks": stats["tasks"]}
 
 
 def bench_serve(cb, n: int, rates) -> dict:

@@ -67,7 +67,8 @@ class ServerOpts(ctypes.Structure):
     _fields_ = [("memory_budget", ctypes.c_size_t), ("max_active", ctypes.c_int), ("chunk_steps", ctypes.c_int),
                 ("temporal_steps", ctypes.c_int), ("tile_rows", ctypes.c_int), ("per_request", ctypes.c_int),
                 ("task_capacity", ctypes.c_int), ("spin_limit", ctypes.c_longlong),
-                ("fail_alloc_at", ctypes.c_longlong), ("round_cells", ctypes.c_double)]
+                ("fail_alloc_at", ctypes.c_longlong), ("round_cells", ctypes.c_double),
+                ("direct_cells", ctypes.c_longlong)]
 
 
 class Request(ctypes.Structure):
@@ -86,7 +87,8 @@ class RequestStatus(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
                 ("rounds", ctypes.c_int64), ("cell_updates", ctypes.c_double), ("used_bytes", ctypes.c_int64),
-                ("budget_bytes", ctypes.c_int64), ("now_s", ctypes.c_double)]
+                ("budget_bytes", ctypes.c_int64), ("now_s", ctypes.c_double), ("plan_s", ctypes.c_double),
+                ("wait_s", ctypes.c_double), ("tasks", ctypes.c_int64)]
 
 
 REQ_QUEUED, REQ_ACTIVE, REQ_DONE, REQ_FAILED = 0, 1, 2, 3

@@ -10,7 +10,14 @@
 //           the device.
 //   round   every active request advances up to chunk_steps generations in
 //           one replay of a batch engine's graph (cb2_batch.cu): one
-//           persistent kernel over all their tasks.  Optionally (round_cells)
+//           persistent kernel over all their tasks.  Requests of at least
+//           direct_cells cells instead advance through the single-grid strip
+//           kernels (cb2_grid_run's plan: up to 32 generations per HBM round
+//           trip, one CTA of several warps per strip) on side streams (each
+//           request keeps one, so its passes stay in order; several requests'
+//           passes run side by side), so their passes fill the SMs that the
+//           batch kernel's tail leaves idle; a round is retired when its work
+//           on every stream has passed.  Optionally (round_cells)
 //           a request's share is sized so that a round holds about that many
 //           cell-updates -- more generations for small grids, fewer for big
 //           ones -- still capped at chunk_steps.
@@ -24,8 +31,9 @@
 // round, and their work overlaps on the device with the requests already in
 // flight.  State stays resident between rounds.  With per_request = 1 the
 // same loop runs the plain path instead: one request at a time, its
-// generations launched as one sequence of strip passes (cb2_grid_run's
-// path), which is what a traverser per request does.
+// generations launched as one sequence of strip passes with the library's
+// default plan (cb2_grid_run's path), which is what a traverser per request
+// does.
 //
 // Failures are per request: an allocation that fails (or the test hook
 // fail_alloc_at) fails that request with CB2_ENOMEM; a round whose bounded
@@ -54,8 +62,11 @@ namespace {
 
 using clock_t_ = std::chrono::steady_clock;
 
+constexpr int kDirectStreams = 4;  // side streams for the strip passes of large requests
+
 struct request_state {
     int64_t id = 0;
+    int side = 0;  // side stream of a large request
     cb2_request req{};
     std::vector<uint64_t> thr;
     int state = CB2_REQ_QUEUED;
@@ -74,7 +85,9 @@ struct request_state {
 // A round queued on the GPU.
 struct round_rec {
     int engine = 0;
-    cudaEvent_t done = nullptr;
+    bool batched = false;  // the round launched the engine's batch kernel
+    cudaEvent_t done = nullptr;         // main stream: batch kernel and its results
+    cudaEvent_t done_direct[kDirectStreams] = {};  // side streams: strip passes and their results
     std::vector<request_state*> members;
     std::vector<request_state*> finishing;
     double cells = 0;
@@ -87,6 +100,10 @@ struct server_impl {
     int device = 0;
     clock_t_::time_point t0;
     cudaStream_t stream = nullptr;
+    cudaStream_t direct[kDirectStreams] = {};  // strip passes of the large requests
+    cudaEvent_t ev_fork = nullptr;  // main stream -> side streams, after a large request's initialisation
+    bool direct_fork_needed = false;
+    int next_side = 0;
     cudaMemPool_t pool = nullptr;
     unsigned long long* d_sums = nullptr;  // 16 checksum sums, then the conversion flag
     unsigned long long* h_sums = nullptr;
@@ -126,7 +143,38 @@ struct server_impl {
     bool admit_locked(std::vector<request_state*>& newly);
     int init_grid(request_state* r);
     int retire(request_state* r);
+    bool is_direct(const request_state* r) const {
+        return opts.direct_cells > 0 && (double)r->req.x_size * (double)r->req.y_size >= (double)opts.direct_cells;
+    }
+    cudaError_t enqueue_result(request_state* r, cudaStream_t s);
+    cudaEvent_t take_event();
+    bool round_passed(const round_rec& rr) {
+        if (cudaEventQuery(rr.done) != cudaSuccess) return false;
+        for (cudaEvent_t ev : rr.done_direct)
+            if (ev && cudaEventQuery(ev) != cudaSuccess) return false;
+        return true;
+    }
+    void sync_round(const round_rec& rr) {
+        cudaEventSynchronize(rr.done);
+        for (cudaEvent_t ev : rr.done_direct)
+            if (ev) cudaEventSynchronize(ev);
+    }
+    void sync_direct() {
+        for (cudaStream_t s : direct)
+            if (s) cudaStreamSynchronize(s);
+    }
 };
+
+cudaEvent_t server_impl::take_event() {
+    if (spare_events.empty()) {
+        cudaEvent_t ev = nullptr;
+        cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        return ev;
+    }
+    cudaEvent_t ev = spare_events.back();
+    spare_events.pop_back();
+    return ev;
+}
 
 int server_impl::alloc_grid(request_state* r) {
     ++allocs;
@@ -254,8 +302,7 @@ bool server_impl::admit_locked(std::vector<request_state*>& newly) {
 void server_impl::run_one(request_state* r) {
     uint32_t* const bufs[2] = {r->grid.buf[0], r->grid.buf[1]};
     int res = 0;
-    cb2_tuning t{opts.temporal_steps, 0, 0, 0, 0};
-    int rc = run_chunks(r->grid.g, bufs, 0, r->req.steps, &t, stream, &res);
+    int rc = run_chunks(r->grid.g, bufs, 0, r->req.steps, nullptr, stream, &res);  // the default plan
     if (rc) {
         finish(r, rc, cb2_last_error());
         return;
@@ -271,53 +318,108 @@ void server_impl::run_one(request_state* r) {
     finish(r, rc, rc ? cb2_last_error() : "");
 }
 
+// Checksum (and, if asked, cells) of a request whose last generation is
+// queued on `s`, into its slot; read by retire_round after the round's event.
+cudaError_t server_impl::enqueue_result(request_state* r, cudaStream_t s) {
+    const grid_geom& g = r->grid.g;
+    const uint32_t* cur = r->grid.buf[r->grid.cur];
+    unsigned long long* sums = d_slots + 16 * (size_t)r->slot;
+    cudaError_t ce = cudaMemsetAsync(sums, 0, 16 * sizeof(unsigned long long), s);
+    if (ce == cudaSuccess) ce = launch_checksum(g, cur, nullptr, 0, sums, s);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(h_slots + 16 * (size_t)r->slot, sums, 16 * sizeof(unsigned long long),
+                             cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess && r->req.host_result) {
+        const size_t cells = (size_t)g.x_size * (size_t)g.y_size;
+        void* tmp = nullptr;
+        ce = cudaMallocFromPoolAsync(&tmp, cells, pool, s);
+        if (ce == cudaSuccess) ce = launch_unpack_cells(g, cur, tmp, 1, s);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(r->req.host_result, tmp, cells, cudaMemcpyDeviceToHost, s);
+        if (tmp) cudaFreeAsync(tmp, s);
+    }
+    return ce;
+}
+
 void server_impl::launch_round() {
     const int e = next_engine;
-    if (!engine_ready[e]) {
-        int rc = engs[e].init(opts.task_capacity, opts.max_active, tiling.temporal_steps, opts.spin_limit);
-        if (rc) {
-            const std::string msg = cb2_last_error();
-            for (request_state* r : active) finish(r, rc, msg);
-            active.clear();
-            return;
-        }
-        engine_ready[e] = true;
-    }
-    batch_engine& eng = engs[e];
     // Shares: about round_cells cell-updates over the requests with work left.
     std::vector<request_state*> todo;
     for (request_state* r : active)
         if (r->planned < r->req.steps) todo.push_back(r);
     if (todo.empty()) return;
     const int K = tiling.temporal_steps;
-    const double share = opts.round_cells > 0 ? opts.round_cells / (double)todo.size() : 1e300;
+    const double share = opts.round_cells > 0 ? opts.round_cells / (double)todo.size() : 0.0;
     std::vector<batch_item> items;
-    std::vector<request_state*> in_round;
+    std::vector<request_state*> in_round;  // batch kernel members, in item order
+    std::vector<std::pair<request_state*, int64_t>> direct_items;
     const size_t n = todo.size();
     for (size_t j = 0; j < n; ++j) {
         request_state* r = todo[(rot + j) % n];
         const int64_t left = r->req.steps - r->planned;
         const double cells = (double)r->req.x_size * (double)r->req.y_size;
-        int64_t steps = (int64_t)(share / cells) / K * K;
-        steps = std::max<int64_t>(steps, K);
-        steps = std::min<int64_t>(steps, opts.chunk_steps);
+        int64_t steps = opts.chunk_steps;
+        if (share > 0) {  // clamp in floating point: the quotient can exceed any integer
+            const double fit = std::min(share / cells, (double)opts.chunk_steps);
+            steps = std::max<int64_t>((int64_t)fit / K * K, K);
+        }
         steps = std::min<int64_t>(steps, left);
-        items.push_back(batch_item{&r->grid, steps, r->grid.cur});
-        in_round.push_back(r);
+        if (is_direct(r)) {
+            direct_items.push_back({r, steps});
+        } else {
+            items.push_back(batch_item{&r->grid, steps, r->grid.cur});
+            in_round.push_back(r);
+        }
     }
     rot = n ? (rot + 1) % n : 0;
-    int rc = eng.build(items, tiling);
-    while (rc == CB2_ENOMEM && items.size() > 1) {  // too many tasks: the rest wait for the next round
-        items.pop_back();
-        in_round.pop_back();
-        rc = eng.build(items, tiling);
+    int rc = CB2_OK;
+    if (!items.empty() && !engine_ready[e]) {
+        rc = engs[e].init(opts.task_capacity, opts.max_active, tiling.temporal_steps, opts.spin_limit);
+        if (rc) {
+            const std::string msg = cb2_last_error();
+            for (request_state* r : in_round) finish(r, rc, msg);
+            active.erase(std::remove_if(active.begin(), active.end(), [](request_state* r) { return r->settled; }),
+                         active.end());
+            return;
+        }
+        engine_ready[e] = true;
     }
-    if (!rc) rc = eng.upload(stream);
-    if (!rc) rc = eng.launch(stream);
-    if (!rc) rc = eng.read_error_async(stream);
+    batch_engine& eng = engs[e];
+    if (!items.empty()) {
+        rc = eng.build(items, tiling);
+        while (rc == CB2_ENOMEM && items.size() > 1) {  // too many tasks: the rest wait for the next round
+            items.pop_back();
+            in_round.pop_back();
+            rc = eng.build(items, tiling);
+        }
+    }
     round_rec rr;
     rr.engine = e;
     rr.members = in_round;
+    for (auto& d : direct_items) rr.members.push_back(d.first);
+    // A large request's passes follow each other on its side stream; the side
+    // streams wait for the main stream only after a large request's state was
+    // initialised there.
+    cudaError_t ce = cudaSuccess;
+    if (!rc && !direct_items.empty() && direct_fork_needed) {
+        direct_fork_needed = false;
+        ce = cudaEventRecord(ev_fork, stream);
+        for (int i = 0; i < kDirectStreams && ce == cudaSuccess; ++i) ce = cudaStreamWaitEvent(direct[i], ev_fork, 0);
+        if (ce != cudaSuccess) {
+            cudaGetLastError();
+            rc = CB2_ECUDA;
+            set_error(std::string("round fork: ") + cudaGetErrorString(ce));
+        }
+    }
+    if (!rc && !items.empty()) {
+        rc = eng.upload(stream);
+        if (!rc) rc = eng.launch(stream);
+        if (!rc) rc = eng.read_error_async(stream);
+        if (!rc) {
+            rr.batched = true;
+            std::lock_guard<std::mutex> lock(mu);
+            stats.tasks += eng.ntasks;
+        }
+    }
     if (!rc) {
         for (size_t i = 0; i < in_round.size(); ++i) {
             request_state* r = in_round[i];
@@ -325,25 +427,8 @@ void server_impl::launch_round() {
             r->planned += items[i].steps;
             rr.cells += (double)r->req.x_size * r->req.y_size * items[i].steps;
             if (r->planned < r->req.steps) continue;
-            // last round of r: checksum (and cells) follow in stream order
-            rr.finishing.push_back(r);
-            const grid_geom& g = r->grid.g;
-            const uint32_t* cur = r->grid.buf[r->grid.cur];
-            unsigned long long* sums = d_slots + 16 * (size_t)r->slot;
-            cudaError_t ce = cudaMemsetAsync(sums, 0, 16 * sizeof(unsigned long long), stream);
-            if (ce == cudaSuccess) ce = launch_checksum(g, cur, nullptr, 0, sums, stream);
-            if (ce == cudaSuccess)
-                ce = cudaMemcpyAsync(h_slots + 16 * (size_t)r->slot, sums, 16 * sizeof(unsigned long long),
-                                     cudaMemcpyDeviceToHost, stream);
-            if (ce == cudaSuccess && r->req.host_result) {
-                const size_t cells = (size_t)g.x_size * (size_t)g.y_size;
-                void* tmp = nullptr;
-                ce = cudaMallocFromPoolAsync(&tmp, cells, pool, stream);
-                if (ce == cudaSuccess) ce = launch_unpack_cells(g, cur, tmp, 1, stream);
-                if (ce == cudaSuccess)
-                    ce = cudaMemcpyAsync(r->req.host_result, tmp, cells, cudaMemcpyDeviceToHost, stream);
-                if (tmp) cudaFreeAsync(tmp, stream);
-            }
+            rr.finishing.push_back(r);  // last round of r: checksum (and cells) follow in stream order
+            ce = enqueue_result(r, stream);
             if (ce != cudaSuccess) {
                 cudaGetLastError();
                 rc = CB2_ECUDA;
@@ -352,15 +437,43 @@ void server_impl::launch_round() {
             }
         }
     }
-    if (!rc) {
-        if (spare_events.empty()) {
-            cudaEvent_t ev;
-            cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
-            spare_events.push_back(ev);
+    if (!rc && !direct_items.empty()) {
+        bool used[kDirectStreams] = {};
+        for (auto& d : direct_items) {
+            request_state* r = d.first;
+            cudaStream_t side = direct[r->side];
+            used[r->side] = true;
+            uint32_t* const bufs[2] = {r->grid.buf[0], r->grid.buf[1]};
+            int res = r->grid.cur;
+            rc = run_chunks(r->grid.g, bufs, r->grid.cur, d.second, nullptr, side, &res);
+            if (rc) break;
+            r->grid.cur = res;
+            r->planned += d.second;
+            rr.cells += (double)r->req.x_size * r->req.y_size * d.second;
+            if (r->planned < r->req.steps) continue;
+            rr.finishing.push_back(r);
+            ce = enqueue_result(r, side);
+            if (ce != cudaSuccess) {
+                cudaGetLastError();
+                rc = CB2_ECUDA;
+                set_error(std::string("request result: ") + cudaGetErrorString(ce));
+                break;
+            }
         }
-        rr.done = spare_events.back();
-        spare_events.pop_back();
-        cudaError_t ce = cudaEventRecord(rr.done, stream);
+        for (int i = 0; i < kDirectStreams && !rc; ++i) {
+            if (!used[i]) continue;
+            rr.done_direct[i] = take_event();
+            ce = cudaEventRecord(rr.done_direct[i], direct[i]);
+            if (ce != cudaSuccess) {
+                cudaGetLastError();
+                rc = CB2_ECUDA;
+                set_error(std::string("round event: ") + cudaGetErrorString(ce));
+            }
+        }
+    }
+    if (!rc) {
+        rr.done = take_event();
+        ce = cudaEventRecord(rr.done, stream);
         if (ce != cudaSuccess) {
             cudaGetLastError();
             rc = CB2_ECUDA;
@@ -369,21 +482,26 @@ void server_impl::launch_round() {
     }
     if (rc) {
         // A failed launch: the round's requests fail, the rest go on.
+        sync_direct();
         cudaStreamSynchronize(stream);
         const std::string msg = cb2_last_error();
-        for (request_state* r : in_round) finish(r, rc, msg);
+        for (request_state* r : rr.members) finish(r, rc, msg);
         active.erase(std::remove_if(active.begin(), active.end(), [](request_state* r) { return r->settled; }),
                      active.end());
         if (rr.done) spare_events.push_back(rr.done);
+        for (cudaEvent_t ev : rr.done_direct)
+            if (ev) spare_events.push_back(ev);
         return;
     }
-    next_engine ^= 1;
+    if (rr.batched) next_engine ^= 1;
     inflight.push_back(std::move(rr));
 }
 
 void server_impl::retire_round(round_rec& rr) {
-    const int rc = engs[rr.engine].error_seen();
+    const int rc = rr.batched ? engs[rr.engine].error_seen() : CB2_OK;
     spare_events.push_back(rr.done);
+    for (cudaEvent_t ev : rr.done_direct)
+        if (ev) spare_events.push_back(ev);
     if (rc) {
         // a bounded wait ran out: the round's requests hold no valid state
         const std::string msg = cb2_last_error();
@@ -428,13 +546,18 @@ void server_impl::loop() {
                 finish(r, rc, cb2_last_error());
                 continue;
             }
+            if (is_direct(r)) {
+                direct_fork_needed = true;
+                r->side = next_side;
+                next_side = (next_side + 1) % kDirectStreams;
+            }
             if (opts.per_request)
                 run_one(r);
             else
                 active.push_back(r);
         }
         if (opts.per_request) continue;
-        while (!inflight.empty() && cudaEventQuery(inflight.front().done) == cudaSuccess) {
+        while (!inflight.empty() && round_passed(inflight.front())) {
             retire_round(inflight.front());
             inflight.pop_front();
         }
@@ -445,11 +568,21 @@ void server_impl::loop() {
                 break;
             }
         if (work && inflight.size() < 2) {
+            const double t_plan = now();
             launch_round();
+            const double dt = now() - t_plan;
+            std::lock_guard<std::mutex> lock(mu);
+            stats.plan_s += dt;
             continue;
         }
         if (!inflight.empty()) {
-            cudaEventSynchronize(inflight.front().done);
+            const double t_wait = now();
+            sync_round(inflight.front());
+            {
+                const double dt = now() - t_wait;
+                std::lock_guard<std::mutex> lock(mu);
+                stats.wait_s += dt;
+            }
             retire_round(inflight.front());
             inflight.pop_front();
             continue;
@@ -464,6 +597,7 @@ void server_impl::loop() {
                          active.end());
         }
     }
+    sync_direct();
     cudaStreamSynchronize(stream);
     while (!inflight.empty()) {
         retire_round(inflight.front());
@@ -502,6 +636,10 @@ int cb2_server_create(const cb2_server_opts* opts, cb2_server** out) {
     if (m.opts.temporal_steps <= 0) m.opts.temporal_steps = 8;
     if (m.opts.tile_rows <= 0) m.opts.tile_rows = 128;
     if (m.opts.task_capacity <= 0) m.opts.task_capacity = 1 << 20;
+    // Measured on the served mix (sides up to 16384): with 128-generation
+    // rounds the batch kernel beats side-stream strip passes for every grid
+    // of that mix, so only larger grids take them by default.
+    if (m.opts.direct_cells == 0) m.opts.direct_cells = 1ll << 28;
     m.tiling.temporal_steps = m.opts.temporal_steps;
     m.tiling.tile_rows = m.opts.tile_rows;
     m.t0 = clock_t_::now();
@@ -511,6 +649,9 @@ int cb2_server_create(const cb2_server_opts* opts, cb2_server** out) {
     if (m.opts.memory_budget == 0)
         m.opts.memory_budget = std::min<size_t>((size_t)150 << 30, free_b / 10 * 8);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&m.stream, cudaStreamNonBlocking);
+    for (int i = 0; i < kDirectStreams && e == cudaSuccess; ++i)
+        e = cudaStreamCreateWithFlags(&m.direct[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&m.ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) {
         cudaMemPoolProps props{};
         props.allocType = cudaMemAllocationTypePinned;
@@ -531,6 +672,9 @@ int cb2_server_create(const cb2_server_opts* opts, cb2_server** out) {
         cudaGetLastError();
         set_error(std::string("server setup: ") + cudaGetErrorString(e));
         if (m.stream) cudaStreamDestroy(m.stream);
+        for (cudaStream_t d : m.direct)
+            if (d) cudaStreamDestroy(d);
+        if (m.ev_fork) cudaEventDestroy(m.ev_fork);
         if (m.pool) cudaMemPoolDestroy(m.pool);
         cudaFree(m.d_sums);
         cudaFreeHost(m.h_sums);
@@ -659,6 +803,7 @@ int cb2_server_destroy(cb2_server* s) {
         m.cv_work.notify_all();
     }
     if (m.thread.joinable()) m.thread.join();
+    m.sync_direct();
     cudaStreamSynchronize(m.stream);
     for (int e = 0; e < 2; ++e)
         if (m.engine_ready[e]) m.engs[e].release();
@@ -668,6 +813,8 @@ int cb2_server_destroy(cb2_server* s) {
     cudaFree(m.d_slots);
     cudaFreeHost(m.h_slots);
     cudaMemPoolDestroy(m.pool);
+    cudaEventDestroy(m.ev_fork);
+    for (cudaStream_t d : m.direct) cudaStreamDestroy(d);
     cudaStreamDestroy(m.stream);
     delete s;
     return CB2_OK;

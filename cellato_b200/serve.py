@@ -19,9 +19,9 @@ class Server:
 
     def __init__(self, memory_budget: int = 0, max_active: int = 0, chunk_steps: int = 0, temporal_steps: int = 0,
                  tile_rows: int = 0, per_request: bool = False, task_capacity: int = 0, spin_limit: int = 0,
-                 fail_alloc_at: int = 0, round_cells: float = 0.0):
+                 fail_alloc_at: int = 0, round_cells: float = 0.0, direct_cells: int = 0):
         opts = _abi.ServerOpts(memory_budget, max_active, chunk_steps, temporal_steps, tile_rows, int(per_request),
-                               task_capacity, spin_limit, fail_alloc_at, round_cells)
+                               task_capacity, spin_limit, fail_alloc_at, round_cells, direct_cells)
         h = ctypes.c_void_p()
         check(lib.cb2_server_create(ctypes.byref(opts), ctypes.byref(h)), "server create")
         self._h = h

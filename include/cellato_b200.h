@@ -236,6 +236,10 @@ typedef struct cb2_server_opts {
     long long fail_alloc_at; /* test hook: the n-th state allocation fails (0 = never)  */
     double round_cells;      /* if > 0: cell-updates a round aims at, shared by its
                                 requests (0 = every request takes chunk_steps)        */
+    long long direct_cells;  /* requests of at least this many cells advance through the
+                                single-grid strip kernels (cb2_grid_run's plan) on a
+                                second stream in each round, beside the batch kernel
+                                (0 = 2^28, e.g. 16384 x 16384; negative = never)       */
 } cb2_server_opts;
 
 typedef struct cb2_request {
@@ -268,6 +272,9 @@ typedef struct cb2_server_stats {
     double cell_updates;
     int64_t used_bytes, budget_bytes;
     double now_s;
+    double plan_s;     /* server-thread seconds spent planning and queueing rounds   */
+    double wait_s;     /* server-thread seconds blocked on the GPU                   */
+    int64_t tasks;     /* batch-kernel tasks run so far                              */
 } cb2_server_stats;
 
 int cb2_server_create(const cb2_server_opts* opts, cb2_server** out);

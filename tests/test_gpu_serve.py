@@ -119,3 +119,27 @@ def test_concurrent_submitters(cuda):
         srv.drain(120)
         for (a, x, y, s, seed), rid in zip(mix, ids):
             assert srv.status(rid)["checksum"] == oracle_checksum(a, x, y, s, seed)
+
+
+@pytest.mark.parametrize("direct_cells", [1, 2048, -1])
+def test_large_requests_through_the_strip_kernels_match_the_oracle(cuda, direct_cells):
+    # direct_cells = 1: every request advances by strip passes on the second stream;
+    # 2048: a mix of batch-kernel and strip-pass requests; -1: none of them.
+    mix = specs(24, 7)
+    with cb.Server(chunk_steps=16, direct_cells=direct_cells) as srv:
+        ids = [srv.submit(a, x, y, s, seed, PROBS[a]) for (a, x, y, s, seed) in mix]
+        srv.drain(120)
+        got = [srv.wait(i)["checksum"] for i in ids]
+    for (a, x, y, s, seed), ck in zip(mix, got):
+        assert ck == oracle_checksum(a, x, y, s, seed), (a, x, y, s, direct_cells)
+
+
+def test_large_request_cells_out_through_the_strip_kernels(cuda):
+    with cb.Server(chunk_steps=8, direct_cells=1000) as srv:
+        jobs = []
+        for (a, x, y, s, seed) in specs(8, 9):
+            cells = O.init_cells(x, y, seed, O.thresholds(PROBS[a]))
+            jobs.append((a, cells, s, srv.submit(a, x, y, s, cells=cells, want_cells=True)))
+        srv.drain(120)
+        for a, cells, s, rid in jobs:
+            assert (srv.result_cells(rid) == O.run_standard(a, cells, s)).all()
