@@ -107,8 +107,12 @@ _SIGNATURES = {
     "cb2_automaton_lookup": (ctypes.c_int, [ctypes.c_char_p]),
     "cb2_automaton_info": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
                                           ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "cb2_automaton_count": (ctypes.c_int, []),
+    "cb2_automaton_values": (ctypes.c_int, [ctypes.c_int, _i64p, ctypes.c_int]),
     "cb2_run_bit_planes": (ctypes.c_int, [ctypes.c_int, _vpp, _vpp, _i64, _i64, _i64, _tp, _vp,
                                           ctypes.POINTER(ctypes.c_int)]),
+    "cb2_run_bit_planes_at": (ctypes.c_int, [ctypes.c_int, _vpp, _vpp, _i64, _i64, _i64, _i64, ctypes.c_uint64, _tp,
+                                             _vp, ctypes.POINTER(ctypes.c_int)]),
     "cb2_run_bit_planes_in_place": (ctypes.c_int, [ctypes.c_int, _vpp, _i64, _i64, _i64, _tp, _vp]),
     "cb2_band_pass": (ctypes.c_int, [ctypes.c_int, _vpp, _vpp, _i64, _i64, _i64, _i64, ctypes.c_int, _tp, _vp]),
     "cb2_fill_random_planes": (ctypes.c_int, [ctypes.c_int, _vpp, _i64, _i64, _i64, _i64, ctypes.c_uint64, _u64p,
@@ -125,6 +129,8 @@ _SIGNATURES = {
     "cb2_grid_checksum": (ctypes.c_int, [_vp, _i64p, ctypes.c_int, _u64p, _vp]),
     "cb2_grid_planes": (ctypes.c_int, [_vp, _vpp, ctypes.POINTER(ctypes.c_int), _i64p]),
     "cb2_grid_time_step": (_i64, [_vp]),
+    "cb2_grid_set_seed": (ctypes.c_int, [_vp, ctypes.c_uint64]),
+    "cb2_grid_set_time_step": (ctypes.c_int, [_vp, _i64]),
     "cb2_batch_create": (ctypes.c_int, [_vpp, _i64p, ctypes.c_int, ctypes.POINTER(BatchOpts), ctypes.POINTER(_vp)]),
     "cb2_batch_destroy": (ctypes.c_int, [_vp]),
     "cb2_batch_run": (ctypes.c_int, [_vp, _vp]),

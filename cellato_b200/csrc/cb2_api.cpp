@@ -41,17 +41,36 @@ static int cuda_fail(cudaError_t e, const char* what) {
         if (e_ != cudaSuccess) return cuda_fail(e_, #call);                                                            \
     } while (0)
 
-static const char* const kNames[kNumAutomata] = {"game-of-life", "wire", "excitable"};
-static const int kStates[kNumAutomata] = {2, 4, 8};
+// The hand-written networks (cb2_rules.cuh).  Their dictionaries list the
+// states in enum order (game_of_life/config.hpp:21, wire/config.hpp:21-24,
+// excitable/config.hpp:21-28), so index and state value coincide.
+static const int64_t kIdentity[32] = {0,  1,  2,  3,  4,  5,  6,  7,  8,  9,  10, 11, 12, 13, 14, 15,
+                                      16, 17, 18, 19, 20, 21, 22, 23, 24, 25, 26, 27, 28, 29, 30, 31};
+static const automaton_desc kBuiltin[kNumBuiltin] = {
+    {"game-of-life", 1, 2, kIdentity}, {"wire", 2, 4, kIdentity}, {"excitable", 3, 8, kIdentity}};
+
+int automaton_count() { return kNumBuiltin + generic_count(); }
+
+const automaton_desc* automaton_at(int id) {
+    if (id >= 0 && id < kNumBuiltin) return &kBuiltin[id];
+    if (id >= kNumBuiltin && id < automaton_count()) return generic_desc(id - kNumBuiltin);
+    return nullptr;
+}
+
+int planes_of(int automaton) {
+    const automaton_desc* d = automaton_at(automaton);
+    return d ? d->planes : -1;
+}
 
 const char* name_of(int automaton) {
-    return automaton >= 0 && automaton < kNumAutomata ? kNames[automaton] : nullptr;
+    const automaton_desc* d = automaton_at(automaton);
+    return d ? d->name : nullptr;
 }
 
 int find_automaton(const char* name) {
     if (!name) return -1;
-    for (int i = 0; i < kNumAutomata; ++i)
-        if (std::strcmp(name, kNames[i]) == 0) return i;
+    for (int i = 0; i < automaton_count(); ++i)
+        if (std::strcmp(name, name_of(i)) == 0) return i;
     return -1;
 }
 
@@ -96,7 +115,14 @@ static bool valid_k(int k) { return k == 1 || k == 2 || k == 4 || k == 8 || k ==
 
 // Default (K, V, L, rows per step) per automaton, the fastest plans measured
 // on B200 at the headline sizes; cb2_autotune replaces them per size.
-static const int kDefaultPlan[kNumAutomata][4] = {{32, 2, 16, 4}, {32, 1, 16, 4}, {32, 2, 16, 4}};
+static const int kDefaultPlan[kNumBuiltin][4] = {{32, 2, 16, 4}, {32, 1, 16, 4}, {32, 2, 16, 4}};
+// Lowered DSL automata: a window of 3P words per row and level keeps the
+// register count in check only for short chains.
+static const int kDefaultDslPlan[4] = {8, 1, 2, 2};
+
+static const int* default_plan(int automaton) {
+    return automaton < kNumBuiltin ? kDefaultPlan[automaton] : kDefaultDslPlan;
+}
 
 // Fills every 0 field of `t` for a grid of geometry g.
 int resolve_plan(const grid_geom& g, const cb2_tuning* t, run_plan* plan) {
@@ -104,13 +130,19 @@ int resolve_plan(const grid_geom& g, const cb2_tuning* t, run_plan* plan) {
     if (t) want = *t;
     cb2_tuning tuned{0, 0, 0, 0, 0};
     const bool have_tuned = tuned_entry(g.automaton, g.x_size, g.y_size, &tuned);
-    const int* def = kDefaultPlan[g.automaton];
+    const int* def = default_plan(g.automaton);
     const int k = want.temporal_steps ? want.temporal_steps : (have_tuned ? tuned.temporal_steps : def[0]);
     if (!valid_k(k))
         return fail(CB2_EINVAL, "temporal_steps must be 1, 2, 4, 8, 16 or 32 (got " + std::to_string(k) + ")");
     const bool tuned_k = have_tuned && tuned.temporal_steps == k;
     int v = want.words_per_lane;
-    if (!v) v = tuned_k ? tuned.words_per_lane : (g.wd <= 30 ? 1 : (k == def[0] ? def[1] : 2));
+    if (!v) {
+        v = tuned_k ? tuned.words_per_lane : (g.wd <= 30 ? 1 : (k == def[0] ? def[1] : 2));
+        if (!find_variant(g.automaton, k, v, 0)) {  // the automaton's table has no kernel that wide at this K
+            const strip_variant* any = find_variant(g.automaton, k, 0, 0);
+            if (any) v = any->v;
+        }
+    }
     if (v != 1 && v != 2 && v != 4)
         return fail(CB2_EINVAL, "words_per_lane must be 1, 2 or 4 (got " + std::to_string(v) + ")");
     int l = want.levels_per_warp;
@@ -150,6 +182,7 @@ int make_geom(int automaton, int64_t x, int64_t y, grid_geom* g) {
     if (x / 32 > (1 << 30) || y > (1 << 30)) return fail(CB2_EINVAL, "grid too large");
     g->automaton = automaton;
     g->planes = P;
+    g->states = automaton_at(automaton)->states;
     g->x_size = x;
     g->y_size = y;
     g->wd = (int32_t)(x / 32);
@@ -161,7 +194,7 @@ int make_geom(int automaton, int64_t x, int64_t y, grid_geom* g) {
 // Launches `steps` generations from `cur` (buffer index) alternating with
 // the other buffer; returns the index that holds the result.
 int run_chunks(const grid_geom& g, uint32_t* const bufs[2], int cur, int64_t steps, const cb2_tuning* tuning,
-               cudaStream_t stream, int* result) {
+               cudaStream_t stream, int* result, int64_t t0, uint64_t seed) {
     run_plan main_plan;
     int rc = resolve_plan(g, tuning, &main_plan);
     if (rc) return rc;
@@ -176,7 +209,7 @@ int run_chunks(const grid_geom& g, uint32_t* const bufs[2], int cur, int64_t ste
             rc = resolve_plan(g, &t2, &p);
             if (rc) return rc;
         }
-        cudaError_t e = launch_strip_pass(g, bufs[cur], bufs[1 - cur], p, stream);
+        cudaError_t e = launch_strip_pass(g, bufs[cur], bufs[1 - cur], p, stream, t0 + (steps - left), seed);
         if (e != cudaSuccess) return cuda_fail(e, "strip kernel launch");
         cur = 1 - cur;
         left -= p.k;
@@ -203,11 +236,21 @@ int cb2_automaton_lookup(const char* name) {
 }
 
 int cb2_automaton_info(int id, const char** name, int* planes, int* states) {
-    if (id < 0 || id >= kNumAutomata) return fail(CB2_ENOTFOUND, "unknown automaton id " + std::to_string(id));
-    if (name) *name = kNames[id];
-    if (planes) *planes = planes_of(id);
-    if (states) *states = kStates[id];
+    const automaton_desc* d = automaton_at(id);
+    if (!d) return fail(CB2_ENOTFOUND, "unknown automaton id " + std::to_string(id));
+    if (name) *name = d->name;
+    if (planes) *planes = d->planes;
+    if (states) *states = d->states;
     return CB2_OK;
+}
+
+int cb2_automaton_count(void) { return automaton_count(); }
+
+int cb2_automaton_values(int id, int64_t* values, int capacity) {
+    const automaton_desc* d = automaton_at(id);
+    if (!d) return fail(CB2_ENOTFOUND, "unknown automaton id " + std::to_string(id));
+    for (int i = 0; values && i < capacity && i < d->states; ++i) values[i] = d->values[i];
+    return d->states;
 }
 
 int64_t cb2_layout_bytes(int automaton, int layout, int word_bits, int64_t x, int64_t y) {
@@ -243,6 +286,12 @@ int64_t cb2_layout_bytes(int automaton, int layout, int word_bits, int64_t x, in
 
 int cb2_run_bit_planes(int automaton, void* const* a, void* const* b, int64_t x_size, int64_t y_size, int64_t steps,
                        const cb2_tuning* tuning, void* stream, int* result_in_b) {
+    return cb2_run_bit_planes_at(automaton, a, b, x_size, y_size, 0, steps, kDefaultSeed, tuning, stream, result_in_b);
+}
+
+int cb2_run_bit_planes_at(int automaton, void* const* a, void* const* b, int64_t x_size, int64_t y_size,
+                          int64_t time_step, int64_t steps, uint64_t seed, const cb2_tuning* tuning, void* stream,
+                          int* result_in_b) {
     grid_geom g;
     int rc = make_geom(automaton, x_size, y_size, &g);
     if (rc) return rc;
@@ -254,9 +303,10 @@ int cb2_run_bit_planes(int automaton, void* const* a, void* const* b, int64_t x_
             (char*)b[p] - (char*)b[0] != (ptrdiff_t)(p * g.plane_words * 4))
             return fail(CB2_EINVAL, "planes must be consecutive in one allocation (stride = y_size * x_size / 8 bytes)");
     }
+    if (time_step < 0) return fail(CB2_EINVAL, "time_step must be non-negative");
     uint32_t* const bufs[2] = {(uint32_t*)a[0], (uint32_t*)b[0]};
     int res = 0;
-    rc = run_chunks(g, bufs, 0, steps, tuning, (cudaStream_t)stream, &res);
+    rc = run_chunks(g, bufs, 0, steps, tuning, (cudaStream_t)stream, &res, time_step, seed);
     if (rc) return rc;
     if (result_in_b) *result_in_b = res;
     return CB2_OK;
@@ -378,8 +428,8 @@ int cb2_grid_download(cb2_grid* grid, int layout, int word_bits, void* host, siz
 int cb2_grid_fill_random(cb2_grid* grid, uint64_t seed, const uint64_t* thresholds, int n, void* stream) {
     if (!grid) return fail(CB2_EINVAL, "null grid");
     if (n < 0 || n > kMaxThresholds || (n && !thresholds))
-        return fail(CB2_EINVAL, "between 0 and 7 thresholds are supported");
-    if (n >= (1 << grid->g.planes)) return fail(CB2_EINVAL, "more thresholds than the automaton has states - 1");
+        return fail(CB2_EINVAL, "between 0 and " + std::to_string(kMaxThresholds) + " thresholds are supported");
+    if (n >= grid->g.states) return fail(CB2_EINVAL, "more thresholds than the automaton has states - 1");
     for (int i = 1; i < n; ++i)
         if (thresholds[i] < thresholds[i - 1]) return fail(CB2_EINVAL, "thresholds must be non-decreasing");
     cudaError_t e = launch_fill_random(grid->g, grid->buf[grid->cur], seed, thresholds, n, (cudaStream_t)stream);
@@ -392,20 +442,38 @@ int cb2_grid_run(cb2_grid* grid, int64_t steps, const cb2_tuning* tuning, void* 
     if (!grid) return fail(CB2_EINVAL, "null grid");
     if (steps < 0) return fail(CB2_EINVAL, "steps must be non-negative");
     int res = grid->cur;
-    int rc = run_chunks(grid->g, grid->buf, grid->cur, steps, tuning, (cudaStream_t)stream, &res);
+    int rc = run_chunks(grid->g, grid->buf, grid->cur, steps, tuning, (cudaStream_t)stream, &res, grid->time_step,
+                        grid->seed);
     if (rc) return rc;
     grid->cur = res;
     grid->time_step += steps;
     return CB2_OK;
 }
 
+int cb2_grid_set_seed(cb2_grid* grid, uint64_t seed) {
+    if (!grid) return fail(CB2_EINVAL, "null grid");
+    grid->seed = seed;
+    return CB2_OK;
+}
+
+int cb2_grid_set_time_step(cb2_grid* grid, int64_t time_step) {
+    if (!grid || time_step < 0) return fail(CB2_EINVAL, "null grid or negative time_step");
+    grid->time_step = time_step;
+    return CB2_OK;
+}
+
 int cb2_grid_checksum(cb2_grid* grid, const int64_t* values, int n_values, uint64_t out[16], void* stream) {
     if (!grid || !out) return fail(CB2_EINVAL, "null grid or output");
     if (n_values < 0 || n_values > (1 << kMaxPlanes) || (n_values && !values))
-        return fail(CB2_EINVAL, "state_values must hold at most 8 entries");
+        return fail(CB2_EINVAL, "state_values must hold at most " + std::to_string(1 << kMaxPlanes) + " entries");
+    if (!values) {  // the dictionary's own state values, as the reference's standard grid sums them
+        const automaton_desc* d = automaton_at(grid->g.automaton);
+        values = d->values;
+        n_values = d->states;
+    }
     cudaStream_t s = (cudaStream_t)stream;
     CB2_CUDA(cudaMemsetAsync(grid->sums, 0, 16 * sizeof(unsigned long long), s));
-    cudaError_t e = launch_checksum(grid->g, grid->buf[grid->cur], values, values ? n_values : 0, grid->sums, s);
+    cudaError_t e = launch_checksum(grid->g, grid->buf[grid->cur], values, n_values, grid->sums, s);
     if (e != cudaSuccess) return cuda_fail(e, "checksum launch");
     unsigned long long host[16];
     CB2_CUDA(cudaMemcpyAsync(host, grid->sums, sizeof(host), cudaMemcpyDeviceToHost, s));
@@ -452,11 +520,10 @@ int cb2_autotune(int automaton, int64_t x_size, int64_t y_size, double budget_ms
     cb2_grid* grid = nullptr;
     rc = cb2_grid_create(automaton, x_size, y_size, &grid);
     if (rc) return rc;
-    const uint64_t half[1] = {1ull << 52};
-    const uint64_t quarters[3] = {1ull << 51, 2ull << 51, 3ull << 51};
-    const uint64_t eighths[7] = {1ull << 50, 2ull << 50, 3ull << 50, 4ull << 50, 5ull << 50, 6ull << 50, 7ull << 50};
-    const uint64_t* thr = g.planes == 1 ? half : g.planes == 2 ? quarters : eighths;
-    rc = cb2_grid_fill_random(grid, 1, thr, (1 << g.planes) - 1, nullptr);
+    // uniform states: thresholds j * 2^53 / states for j = 1 .. states - 1
+    uint64_t thr[kMaxThresholds];
+    for (int j = 1; j < g.states; ++j) thr[j - 1] = (uint64_t)(((unsigned __int128)j << 53) / (unsigned)g.states);
+    rc = cb2_grid_fill_random(grid, 1, thr, g.states - 1, nullptr);
     if (rc) {
         cb2_grid_destroy(grid);
         return rc;
@@ -538,7 +605,7 @@ int cb2_tuning_save(const char* path) {
     f << "# automaton x_size y_size temporal_steps tile_rows words_per_lane levels_per_warp rows_per_step\n";
     std::lock_guard<std::mutex> lock(g_tune_mu);
     for (auto& kv : g_tune)
-        f << kNames[kv.first.automaton] << ' ' << kv.first.x << ' ' << kv.first.y << ' ' << kv.second.temporal_steps
+        f << name_of(kv.first.automaton) << ' ' << kv.first.x << ' ' << kv.first.y << ' ' << kv.second.temporal_steps
           << ' ' << kv.second.tile_rows << ' ' << kv.second.words_per_lane << ' ' << kv.second.levels_per_warp
           << ' ' << kv.second.rows_per_step << '\n';
     return (int)g_tune.size();
@@ -579,8 +646,10 @@ int cb2_network_ops(int automaton, double* alu, double* shuffles) {
     // Per 32-bit word per generation (cb2_rules.cuh): two funnel shifts for
     // the west/east neighbour words, plus the rule's logic ops; two shuffles
     // per lane per row, shared by the lane's V = 2 words.
-    static const double kLogic[kNumAutomata] = {10, 11, 7};
-    if (automaton < 0 || automaton >= kNumAutomata) return fail(CB2_ENOTFOUND, "unknown automaton");
+    static const double kLogic[kNumBuiltin] = {10, 11, 7};
+    if (automaton >= kNumBuiltin && automaton < automaton_count())
+        return fail(CB2_EINVAL, "no static operation count for a lowered DSL automaton");
+    if (automaton < 0 || automaton >= kNumBuiltin) return fail(CB2_ENOTFOUND, "unknown automaton");
     if (alu) *alu = kLogic[automaton] + 2;
     if (shuffles) *shuffles = 1.0;
     return CB2_OK;

@@ -50,6 +50,12 @@ int cb2_band_pass(int automaton, void* const* in, void* const* out, int64_t x_si
     grid_geom g;
     int rc = make_geom(automaton, x_size, rows_total, &g);
     if (rc) return rc;
+    if (automaton >= kNumBuiltin) {
+        // A lowered DSL rule may read the cells' global row (Margolus blocks,
+        // probability draws); a band pass only knows band-local rows.
+        set_error("row bands run the hand-written networks (game-of-life, wire, excitable) only");
+        return CB2_EINVAL;
+    }
     if ((rc = check_planes(g, in, "input")) || (rc = check_planes(g, out, "output"))) return rc;
     if (row_first < 0 || rows_out < 1 || row_first + rows_out > rows_total) {
         set_error("band rows outside the planes");
@@ -84,7 +90,7 @@ int cb2_fill_random_planes(int automaton, void* const* planes, int64_t x_size, i
     int rc = make_geom(automaton, x_size, rows, &g);
     if (rc) return rc;
     if ((rc = check_planes(g, planes, "output"))) return rc;
-    if (global_rows < 1 || n_thresholds < 0 || n_thresholds > kMaxThresholds || n_thresholds >= (1 << g.planes) ||
+    if (global_rows < 1 || n_thresholds < 0 || n_thresholds > kMaxThresholds || n_thresholds >= g.states ||
         (n_thresholds && !thresholds)) {
         set_error("invalid global rows or thresholds");
         return CB2_EINVAL;

@@ -48,7 +48,8 @@
 namespace cb2 {
 
 constexpr int kBatchWarps = 4;                                  // independent warps per CTA
-constexpr int kBatchSmemWords = kMaxPlanes * 32 * kRingDepth;   // one warp's input ring (V = 1)
+constexpr int kBatchPlanes = 3;                                  // the hand-written networks' largest P
+constexpr int kBatchSmemWords = kBatchPlanes * 32 * kRingDepth;  // one warp's input ring (V = 1)
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
     unsigned v;
@@ -400,6 +401,11 @@ int cb2_batch_create(cb2_grid* const* grids, const int64_t* steps, int n, const 
         if (!grids[i] || steps[i] < 0) {
             delete b;
             return efail(CB2_EINVAL, "null grid or negative steps in batch");
+        }
+        if (grids[i]->g.automaton >= kNumBuiltin) {
+            delete b;
+            return efail(CB2_EINVAL, std::string("the batch kernel runs game-of-life, wire and excitable; '") +
+                                         name_of(grids[i]->g.automaton) + "' advances with cb2_grid_run");
         }
         b->items.push_back(batch_item{grids[i], steps[i], grids[i]->cur});
         const cb2_grid* g = grids[i];

@@ -10,15 +10,17 @@
 
 namespace cb2 {
 
-constexpr int kMaxPlanes = 3;
-constexpr int kNumAutomata = 3;
-constexpr int kMaxThresholds = 7;  // up to 8 states
-constexpr int kRingDepth = 8;  // input rows kept in flight per strip task
+constexpr int kMaxPlanes = 5;       // bit-planes of the largest dictionary (32 states)
+constexpr int kNumBuiltin = 3;      // automata with hand-written networks: ids 0, 1, 2
+constexpr int kMaxThresholds = 31;  // up to 32 states
+constexpr int kRingDepth = 8;       // input rows kept in flight per strip task
+constexpr uint64_t kDefaultSeed = 42;  // run_params::seed
 
 // Geometry of one device grid: P planes of h rows x wd 32-bit words.
 struct grid_geom {
     int automaton;
     int planes;
+    int states;              // dictionary size: indexes >= states are not states
     int64_t x_size, y_size;  // cells
     int32_t wd, h;           // 32-bit words per row, rows
     int64_t plane_words;     // wd * h
@@ -41,21 +43,40 @@ struct strip_variant {
     int smem_bytes;
 };
 
+// The automaton registry: ids 0..2 are the hand-written networks, ids from
+// 3 the DSL automata lowered by cb2_ast.cuh (cb2_generic.cu; absent when the
+// library was built without the Cellato headers).
+struct automaton_desc {
+    const char* name;
+    int planes;
+    int states;
+    const int64_t* values;  // dictionary index -> state value (the checksum sums values)
+};
+int automaton_count();
+const automaton_desc* automaton_at(int id);  // nullptr for an unknown id
 int planes_of(int automaton);
 const char* name_of(int automaton);
 int find_automaton(const char* name);
+// Lowered DSL automata (cb2_generic.cu): how many, and their descriptors and
+// kernels, indexed from 0 (= automaton id kNumBuiltin).
+int generic_count();
+const automaton_desc* generic_desc(int i);
 
-// Launches one K-generation strip pass over a whole grid (in -> out).
+// Launches one K-generation strip pass over a whole grid (in -> out); the
+// input is generation t0 (read by time-dependent rules), seed the run's
+// random seed (read by stochastic rules).
 cudaError_t launch_strip_pass(const grid_geom& g, const uint32_t* in, uint32_t* out, const run_plan& plan,
-                              cudaStream_t stream);
+                              cudaStream_t stream, int64_t t0 = 0, uint64_t seed = kDefaultSeed);
 // The same for output rows [y_base, y_base + rows_out) only (input rows wrap mod g.h).
 cudaError_t launch_strip_window(const grid_geom& g, const uint32_t* in, uint32_t* out, const run_plan& plan,
-                                int y_base, int rows_out, cudaStream_t stream);
+                                int y_base, int rows_out, cudaStream_t stream, int64_t t0 = 0,
+                                uint64_t seed = kDefaultSeed);
 // Strip tasks per column and per row for a plan.
 void strip_counts(const grid_geom& g, int v, int tile_rows, int* nsx, int* nsy);
 // The instantiated kernels of an automaton, and the first one matching a
 // plan (v, l or r of 0 match anything).
 const std::vector<strip_variant>& strip_variants(int automaton);
+const std::vector<strip_variant>& generic_variants(int i);  // of lowered automaton i
 const strip_variant* find_variant(int automaton, int k, int v, int l, int r = 0);
 // Output rows per task so that one launch fills the GPU about once.
 int auto_tile_rows(const grid_geom& g, const strip_variant& sv);
@@ -111,7 +132,7 @@ int resolve_plan(const grid_geom& g, const cb2_tuning* t, run_plan* plan);
 // Launches `steps` generations starting in bufs[cur], alternating between the
 // two buffers; *result is the index of the buffer holding the result.
 int run_chunks(const grid_geom& g, uint32_t* const bufs[2], int cur, int64_t steps, const cb2_tuning* tuning,
-               cudaStream_t stream, int* result);
+               cudaStream_t stream, int* result, int64_t t0 = 0, uint64_t seed = kDefaultSeed);
 
 } // namespace cb2
 
@@ -121,6 +142,7 @@ struct cb2_grid {
     uint32_t* buf[2] = {nullptr, nullptr};  // the double buffer; buf[cur] holds the current generation
     int cur = 0;
     int64_t time_step = 0;
+    uint64_t seed = cb2::kDefaultSeed;  // random seed of stochastic rules
     void* staging = nullptr;  // device copy of a host image for layout conversion
     size_t staging_bytes = 0;
     unsigned* flag = nullptr;  // device error flag of the conversion kernels

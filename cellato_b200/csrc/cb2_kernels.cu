@@ -17,54 +17,13 @@
 
 #include "cb2_internal.h"
 #include "cb2_rules.cuh"
-#include "cb2_pipe.cuh"
+#include "cb2_launch.cuh"
 
 namespace cb2 {
 
 // ---------------------------------------------------------------------------
 // Strip pass: one CTA per strip task, K generations per launch
 // ---------------------------------------------------------------------------
-
-struct strip_launch {
-    const uint32_t* in;
-    uint32_t* out;
-    int64_t plane_words;
-    int32_t wd, h;
-    int32_t nsx, nsy, tile_rows;
-    int32_t y_base, rows_out;  // output rows [y_base, y_base + rows_out)
-};
-
-template <class R, int K, int V, int L, int RPS>
-__global__ void __launch_bounds__(32 * (K / L)) pipe_kernel(strip_launch a) {
-    extern __shared__ __align__(16) uint32_t smem[];
-    constexpr int own = 32 * V - 2;
-    const int task = blockIdx.x;
-    const int sx = task % a.nsx, sy = task / a.nsx;
-    strip_task t;
-    t.in = a.in;
-    t.out = a.out;
-    t.plane_words = a.plane_words;
-    t.wd = a.wd;
-    t.h = a.h;
-    t.x0 = sx * own;
-    t.nx = min(own, a.wd - t.x0);
-    t.y0 = a.y_base + sy * a.tile_rows;
-    t.ny = min(a.tile_rows, a.y_base + a.rows_out - t.y0);
-    if constexpr (RPS > 1)
-        pipe_run_rows<R, K, V, L, kRingDepth, RPS>(t, smem);  // RPS rows per barrier
-    else if constexpr (L == K)
-        warp_run<R, K, V, kRingDepth>(t, strip_geom<V>(t, threadIdx.x & 31), smem);  // one warp, skewed levels
-    else
-        pipe_run<R, K, V, L, kRingDepth>(t, smem);
-}
-
-template <class R, int K, int V, int L, int RPS = 1>
-static strip_variant make_variant() {
-    const int words = RPS > 1  ? pipe_rows_smem_words<R, K, V, L, kRingDepth, RPS>()
-                      : L == K ? warp_smem_words<R, V, kRingDepth>()
-                               : pipe_smem_words<R, K, V, L, kRingDepth>();
-    return strip_variant{K, V, L, RPS, (const void*)pipe_kernel<R, K, V, L, RPS>, 32 * (K / L), 4 * words};
-}
 
 // The instantiated (K, V, L, rows per step) plans; for each (K, V) the first
 // entry is the default levels-per-warp, for each (K, V, L) the first entry
@@ -94,7 +53,8 @@ const std::vector<strip_variant>& strip_variants(int automaton) {
     case 0: return variants_for<game_of_life>();
     case 1: return variants_for<wire>();
     case 2: return variants_for<excitable>();
-    default: return none;
+    default: return automaton >= kNumBuiltin && automaton < automaton_count() ? generic_variants(automaton - kNumBuiltin)
+                                                                               : none;
     }
 }
 
@@ -102,15 +62,6 @@ const strip_variant* find_variant(int automaton, int k, int v, int l, int r) {
     for (const strip_variant& sv : strip_variants(automaton))
         if (sv.k == k && (v == 0 || sv.v == v) && (l == 0 || sv.l == l) && (r == 0 || sv.r == r)) return &sv;
     return nullptr;
-}
-
-int planes_of(int automaton) {
-    switch (automaton) {
-    case 0: return game_of_life::P;
-    case 1: return wire::P;
-    case 2: return excitable::P;
-    default: return -1;
-    }
 }
 
 void strip_counts(const grid_geom& g, int v, int tile_rows, int* nsx, int* nsy) {
@@ -157,7 +108,7 @@ int auto_tile_rows(const grid_geom& g, const strip_variant& sv) {
 }
 
 cudaError_t launch_strip_window(const grid_geom& g, const uint32_t* in, uint32_t* out, const run_plan& plan,
-                                int y_base, int rows_out, cudaStream_t stream) {
+                                int y_base, int rows_out, cudaStream_t stream, int64_t t0, uint64_t seed) {
     const strip_variant* sv = find_variant(g.automaton, plan.k, plan.v, plan.l, plan.r);
     if (!sv || rows_out < 1 || y_base < 0 || y_base + rows_out > g.h) return cudaErrorInvalidValue;
     resident_strip_tasks(*sv);  // sets the kernel's shared-memory attribute once
@@ -170,6 +121,8 @@ cudaError_t launch_strip_window(const grid_geom& g, const uint32_t* in, uint32_t
     a.tile_rows = plan.tile_rows;
     a.y_base = y_base;
     a.rows_out = rows_out;
+    a.t0 = t0;
+    a.seed = seed;
     grid_geom window = g;
     window.h = rows_out;
     strip_counts(window, plan.v, plan.tile_rows, &a.nsx, &a.nsy);
@@ -179,8 +132,8 @@ cudaError_t launch_strip_window(const grid_geom& g, const uint32_t* in, uint32_t
 }
 
 cudaError_t launch_strip_pass(const grid_geom& g, const uint32_t* in, uint32_t* out, const run_plan& plan,
-                              cudaStream_t stream) {
-    return launch_strip_window(g, in, out, plan, 0, g.h, stream);
+                              cudaStream_t stream, int64_t t0, uint64_t seed) {
+    return launch_strip_window(g, in, out, plan, 0, g.h, stream, t0, seed);
 }
 
 // ---------------------------------------------------------------------------
@@ -209,7 +162,7 @@ __global__ void fill_random_kernel(uint32_t* planes, int64_t plane_words, int32_
         int64_t gy = (row0 + y) % global_rows;
         if (gy < 0) gy += global_rows;
         const uint64_t i0 = (uint64_t)(gy * x_size + xw * 32);
-        uint32_t out[kMaxPlanes] = {0, 0, 0};
+        uint32_t out[kMaxPlanes] = {};
 #pragma unroll 4
         for (int j = 0; j < 32; ++j) {
             const uint64_t u = mix64(seed + (i0 + j + 1) * 0x9E3779B97F4A7C15ull) >> 11;
@@ -250,13 +203,13 @@ cudaError_t launch_fill_random(const grid_geom& g, uint32_t* planes, uint64_t se
 
 template <typename cell_t>
 __global__ void pack_cells_kernel(const cell_t* __restrict__ cells, int64_t plane_words, int32_t wd, int64_t x_size,
-                                  int P, uint32_t* __restrict__ planes, unsigned* bad) {
+                                  int P, int states, uint32_t* __restrict__ planes, unsigned* bad) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    const uint32_t max_state = (1u << P) - 1u;
+    const uint32_t max_state = (uint32_t)states - 1u;
     for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < plane_words; w += stride) {
         const int64_t y = w / wd, xw = w - y * wd;
         const cell_t* src = cells + y * x_size + xw * 32;
-        uint32_t out[kMaxPlanes] = {0, 0, 0};
+        uint32_t out[kMaxPlanes] = {};
         bool any_bad = false;
 #pragma unroll
         for (int j = 0; j < 32; ++j) {
@@ -276,7 +229,7 @@ __global__ void unpack_cells_kernel(const uint32_t* __restrict__ planes, int64_t
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < plane_words; w += stride) {
         const int64_t y = w / wd, xw = w - y * wd;
-        uint32_t in[kMaxPlanes] = {0, 0, 0};
+        uint32_t in[kMaxPlanes] = {};
         for (int p = 0; p < P; ++p) in[p] = planes[p * plane_words + w];
         cell_t* dst = cells + y * x_size + xw * 32;
 #pragma unroll
@@ -294,10 +247,10 @@ cudaError_t launch_pack_cells(const grid_geom& g, const void* cells, int cell_by
     const unsigned blocks = grid_for(g.plane_words, 256);
     if (cell_bytes == 1)
         pack_cells_kernel<uint8_t><<<blocks, 256, 0, s>>>((const uint8_t*)cells, g.plane_words, g.wd, g.x_size,
-                                                           g.planes, planes, bad_flag);
+                                                           g.planes, g.states, planes, bad_flag);
     else if (cell_bytes == 4)
         pack_cells_kernel<uint32_t><<<blocks, 256, 0, s>>>((const uint32_t*)cells, g.plane_words, g.wd, g.x_size,
-                                                            g.planes, planes, bad_flag);
+                                                            g.planes, g.states, planes, bad_flag);
     else
         return cudaErrorInvalidValue;
     return cudaGetLastError();
@@ -336,7 +289,7 @@ __global__ void bit_array_to_planes_kernel(const word_t* __restrict__ words, int
         int64_t wi = i0 / cpw;
         int r = (int)(i0 - wi * cpw);
         word_t cur = words[wi];
-        uint32_t out[kMaxPlanes] = {0, 0, 0};
+        uint32_t out[kMaxPlanes] = {};
         for (int j = 0; j < 32; ++j) {
             const uint32_t s = (uint32_t)((cur >> (r * P)) & mask);
 #pragma unroll
@@ -361,7 +314,7 @@ __global__ void planes_to_bit_array_kernel(const uint32_t* __restrict__ planes, 
         const int64_t y = i0 / x_size, x0 = i0 - y * x_size;
         word_t out = 0;
         int64_t pw = -1;
-        uint32_t in[kMaxPlanes] = {0, 0, 0};
+        uint32_t in[kMaxPlanes] = {};
         for (int j = 0; j < cpw; ++j) {
             const int64_t x = x0 + j;
             if ((x >> 5) != pw) {
@@ -489,7 +442,7 @@ __global__ void checksum_kernel(const uint32_t* __restrict__ planes, int64_t pla
         const int64_t yr = k / wd, xw = k - yr * wd;
         const int64_t w = (row_first + yr) * wd + xw;
         const int ty = (int)((global_row0 + yr) / th);
-        uint32_t in[kMaxPlanes] = {0, 0, 0};
+        uint32_t in[kMaxPlanes] = {};
         for (int p = 0; p < P; ++p) in[p] = planes[p * plane_words + w];
         const int64_t x0 = xw * 32, x1 = x0 + 32;
         for (int64_t tx = x0 / tw; tx < 4 && tx * tw < x1; ++tx) {

@@ -89,6 +89,7 @@ __device__ __forceinline__ void slot_write(uint32_t* slot, int lane, const uint3
 // `smem` holds pipe_smem_words<R, K, V, L, DEPTH>() words, 16-byte aligned.
 template <class R, int K, int V, int L, int DEPTH>
 __device__ __forceinline__ void pipe_run(const strip_task& t, uint32_t* smem) {
+    static_assert(!R::kWindow, "window rules run in pipe_run_rows");
     static_assert(K % L == 0, "levels per warp must divide K");
     static_assert(K <= 32, "the one-word halo of a strip covers at most 32 generations");
     static_assert(DEPTH >= 2, "input ring of at least two rows");
@@ -270,8 +271,17 @@ __device__ __forceinline__ void pipe_run_rows(const strip_task& t, uint32_t* sme
         }
 #pragma unroll
         for (int j = 0; j < RPS; j += 2) {
-            strip_push<R, L, V, 0>(s, rows[j], geom.src_l, geom.src_r);
-            strip_push<R, L, V, 1>(s, rows[j + 1], geom.src_l, geom.src_r);
+            if constexpr (R::kWindow) {
+                // warp w's chain receives sweep row RPS*st + j - w*(RPS + L) (warp w-1's
+                // output of the previous step, L rows behind its input)
+                row_ctx rc{t.t0 + (int64_t)warp * L, RPS * st + j - warp * (RPS + L), t.y0 - K, t.h, t.seed};
+                strip_push<R, L, V, 0>(s, rows[j], geom.src_l, geom.src_r, &geom, &rc);
+                rc.sweep += 1;
+                strip_push<R, L, V, 1>(s, rows[j + 1], geom.src_l, geom.src_r, &geom, &rc);
+            } else {
+                strip_push<R, L, V, 0>(s, rows[j], geom.src_l, geom.src_r);
+                strip_push<R, L, V, 1>(s, rows[j + 1], geom.src_l, geom.src_r);
+            }
         }
         if (warp == W - 1) {
             const int r0 = RPS * (st - (W - 1));  // input rows whose results leave now
@@ -302,6 +312,7 @@ constexpr int warp_smem_words() {
 // the row K rows above it: output sweep row s - 2K + 1.
 template <class R, int K, int V, int DEPTH>
 __device__ __forceinline__ void warp_run(const strip_task& t, const lane_geom<V>& geom, uint32_t* smem) {
+    static_assert(!R::kWindow, "window rules run in pipe_run_rows");
     constexpr int P = R::P;
     constexpr int SLOT = P * 32 * V;
     const int lane = threadIdx.x & 31;

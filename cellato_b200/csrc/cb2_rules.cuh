@@ -73,6 +73,7 @@ struct game_of_life {
     static constexpr int P = 1;   // bit-planes of state
     static constexpr int NH = 2;  // planes of the horizontal aggregate
     static constexpr int id = 0;
+    static constexpr bool kWindow = false;  // census network (a window rule sees all planes)
     CB2_HD static uint32_t indicator(const uint32_t (&s)[P]) { return s[0]; }
     CB2_HD static void hagg(uint32_t l, uint32_t c, uint32_t r, uint32_t (&h)[NH]) {
         h[0] = xor3(l, c, r);
@@ -94,6 +95,7 @@ struct wire {
     static constexpr int P = 2;
     static constexpr int NH = 2;
     static constexpr int id = 1;
+    static constexpr bool kWindow = false;
     CB2_HD static uint32_t indicator(const uint32_t (&s)[P]) { return s[0] & ~s[1]; }  // head
     CB2_HD static void hagg(uint32_t l, uint32_t c, uint32_t r, uint32_t (&h)[NH]) {
         h[0] = xor3(l, c, r);
@@ -117,6 +119,7 @@ struct excitable {
     static constexpr int P = 3;
     static constexpr int NH = 1;
     static constexpr int id = 2;
+    static constexpr bool kWindow = false;
     CB2_HD static uint32_t indicator(const uint32_t (&s)[P]) { return s[0] & ~s[1] & ~s[2]; }  // excited
     CB2_HD static void hagg(uint32_t l, uint32_t c, uint32_t r, uint32_t (&h)[NH]) { h[0] = l | c | r; }
     // 0 -> 1 iff any excited neighbour; s -> s+1 for 1..6; 7 -> 0.

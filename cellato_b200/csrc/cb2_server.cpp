@@ -144,6 +144,7 @@ struct server_impl {
     int init_grid(request_state* r);
     int retire(request_state* r);
     bool is_direct(const request_state* r) const {
+        if (r->req.automaton >= kNumBuiltin) return true;  // lowered DSL rules run in the strip kernels only
         return opts.direct_cells > 0 && (double)r->req.x_size * (double)r->req.y_size >= (double)opts.direct_cells;
     }
     cudaError_t enqueue_result(request_state* r, cudaStream_t s);
@@ -302,7 +303,7 @@ bool server_impl::admit_locked(std::vector<request_state*>& newly) {
 void server_impl::run_one(request_state* r) {
     uint32_t* const bufs[2] = {r->grid.buf[0], r->grid.buf[1]};
     int res = 0;
-    int rc = run_chunks(r->grid.g, bufs, 0, r->req.steps, nullptr, stream, &res);  // the default plan
+    int rc = run_chunks(r->grid.g, bufs, 0, r->req.steps, nullptr, stream, &res, 0, r->req.seed);  // the default plan
     if (rc) {
         finish(r, rc, cb2_last_error());
         return;
@@ -445,7 +446,7 @@ void server_impl::launch_round() {
             used[r->side] = true;
             uint32_t* const bufs[2] = {r->grid.buf[0], r->grid.buf[1]};
             int res = r->grid.cur;
-            rc = run_chunks(r->grid.g, bufs, r->grid.cur, d.second, nullptr, side, &res);
+            rc = run_chunks(r->grid.g, bufs, r->grid.cur, d.second, nullptr, side, &res, r->planned, r->req.seed);
             if (rc) break;
             r->grid.cur = res;
             r->planned += d.second;
@@ -699,8 +700,9 @@ int cb2_server_submit(cb2_server* s, const cb2_request* req, int64_t* id) {
         set_error("steps must be non-negative");
         return CB2_EINVAL;
     }
-    if (!req->host_cells && (req->n_thresholds < 0 || req->n_thresholds > kMaxThresholds ||
-                             req->n_thresholds >= (1 << g.planes))) {
+    const int max_thr = (int)(sizeof(req->thresholds) / sizeof(req->thresholds[0]));
+    if (!req->host_cells && (req->n_thresholds < 0 || req->n_thresholds > max_thr ||
+                             req->n_thresholds >= g.states)) {
         set_error("between 0 and (states - 1) thresholds are supported");
         return CB2_EINVAL;
     }

@@ -41,6 +41,29 @@ struct strip_task {
     int32_t h;            // rows
     int32_t x0, nx;       // first own word column, own word count (1 .. 32V-2)
     int32_t y0, ny;       // first output row, output row count (1 .. h - y0)
+    int64_t t0;           // generation of the input (read by rules that depend on time)
+    uint64_t seed;        // random seed of the run (read by stochastic rules)
+};
+
+// Where a lane's 32 cells are, for rules that read it (window rules): the
+// generation the rule is evaluated at, the global row, the 32-bit word
+// column (cells 32*xw .. 32*xw+31) and the run's seed.
+struct cell_ctx {
+    int64_t t;
+    int64_t y;
+    int64_t xw;
+    uint64_t seed;
+};
+
+// Where a row pushed into a level chain sits: its sweep index (sweep row r is
+// grid row y0 - K + r, mod h) and the generation of the chain's first level.
+// Only window rules (ast_rule) read it.
+struct row_ctx {
+    int64_t t;     // generation of the first level of the chain
+    int sweep;     // sweep index of the row entering the first level
+    int y_base;    // grid row of sweep index 0 (y0 - K)
+    int h;         // rows of the grid
+    uint64_t seed;
 };
 
 constexpr unsigned kFullMask = 0xffffffffu;
@@ -108,31 +131,66 @@ struct strip_state {
 // generation.
 template <class R, int K, int V, int Q>
 __device__ __forceinline__ void level_push(strip_state<R, K, V>& s, int g, uint32_t (&row)[V][R::P], int src_l,
-                                           int src_r) {
+                                           int src_r, const lane_geom<V>* geom = nullptr, const row_ctx* rc = nullptr) {
     constexpr int P = R::P, NH = R::NH;
-    uint32_t ind[V];
-#pragma unroll
-    for (int i = 0; i < V; ++i) ind[i] = R::indicator(row[i]);
-    const uint32_t lw = __shfl_sync(kFullMask, ind[V - 1], src_l);
-    const uint32_t rw = __shfl_sync(kFullMask, ind[0], src_r);
-    uint32_t hc[V][NH];
-#pragma unroll
-    for (int i = 0; i < V; ++i) {
-        const uint32_t l = i == 0 ? lw : ind[i - 1];
-        const uint32_t r = i == V - 1 ? rw : ind[i + 1];
-        R::hagg(west_of(l, ind[i]), ind[i], east_of(ind[i], r), hc[i]);
-    }
-    uint32_t nxt[V][P];
-#pragma unroll
-    for (int i = 0; i < V; ++i) R::next(s.h[g][Q][i], s.h[g][1 - Q][i], hc[i], s.c[g][1 - Q][i], nxt[i]);
-#pragma unroll
-    for (int i = 0; i < V; ++i) {
-#pragma unroll
-        for (int k = 0; k < NH; ++k) s.h[g][Q][i][k] = hc[i][k];
+    if constexpr (R::kWindow) {
+        // window rule: (west, centre, east) word of every plane; the AST reads the
+        // 3x3 window and the cells' generation and position
+        uint32_t hc[V][NH];
 #pragma unroll
         for (int p = 0; p < P; ++p) {
-            s.c[g][Q][i][p] = row[i][p];
-            row[i][p] = nxt[i][p];
+            const uint32_t lw = __shfl_sync(kFullMask, row[V - 1][p], src_l);
+            const uint32_t rw = __shfl_sync(kFullMask, row[0][p], src_r);
+#pragma unroll
+            for (int i = 0; i < V; ++i) {
+                const uint32_t l = i == 0 ? lw : row[i - 1][p];
+                const uint32_t r = i == V - 1 ? rw : row[i + 1][p];
+                hc[i][3 * p] = west_of(l, row[i][p]);
+                hc[i][3 * p + 1] = row[i][p];
+                hc[i][3 * p + 2] = east_of(row[i][p], r);
+            }
+        }
+        // level g outputs the row one above its input: sweep index rc->sweep - g - 1
+        int64_t y = ((int64_t)rc->y_base + rc->sweep - g - 1) % rc->h;
+        if (y < 0) y += rc->h;
+        uint32_t nxt[V][P];
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+            const cell_ctx c{rc->t + g, y, geom->col[i], rc->seed};
+            R::next_at(s.h[g][Q][i], s.h[g][1 - Q][i], hc[i], nxt[i], c);
+        }
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+#pragma unroll
+            for (int k = 0; k < NH; ++k) s.h[g][Q][i][k] = hc[i][k];
+#pragma unroll
+            for (int p = 0; p < P; ++p) row[i][p] = nxt[i][p];
+        }
+    } else {
+        uint32_t ind[V];
+#pragma unroll
+        for (int i = 0; i < V; ++i) ind[i] = R::indicator(row[i]);
+        const uint32_t lw = __shfl_sync(kFullMask, ind[V - 1], src_l);
+        const uint32_t rw = __shfl_sync(kFullMask, ind[0], src_r);
+        uint32_t hc[V][NH];
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+            const uint32_t l = i == 0 ? lw : ind[i - 1];
+            const uint32_t r = i == V - 1 ? rw : ind[i + 1];
+            R::hagg(west_of(l, ind[i]), ind[i], east_of(ind[i], r), hc[i]);
+        }
+        uint32_t nxt[V][P];
+#pragma unroll
+        for (int i = 0; i < V; ++i) R::next(s.h[g][Q][i], s.h[g][1 - Q][i], hc[i], s.c[g][1 - Q][i], nxt[i]);
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+#pragma unroll
+            for (int k = 0; k < NH; ++k) s.h[g][Q][i][k] = hc[i][k];
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                s.c[g][Q][i][p] = row[i][p];
+                row[i][p] = nxt[i][p];
+            }
         }
     }
 }
@@ -141,9 +199,10 @@ __device__ __forceinline__ void level_push(strip_state<R, K, V>& s, int g, uint3
 // this row; on return `row` holds the row K rows above it, advanced K
 // generations.
 template <class R, int K, int V, int Q>
-__device__ __forceinline__ void strip_push(strip_state<R, K, V>& s, uint32_t (&row)[V][R::P], int src_l, int src_r) {
+__device__ __forceinline__ void strip_push(strip_state<R, K, V>& s, uint32_t (&row)[V][R::P], int src_l, int src_r,
+                                           const lane_geom<V>* geom = nullptr, const row_ctx* rc = nullptr) {
 #pragma unroll
-    for (int g = 0; g < K; ++g) level_push<R, K, V, Q>(s, g, row, src_l, src_r);
+    for (int g = 0; g < K; ++g) level_push<R, K, V, Q>(s, g, row, src_l, src_r, geom, rc);
 }
 
 // Skewed wavefront step: level g takes the row level g-1 produced in the

@@ -16,7 +16,18 @@ import numpy as np
 from . import _abi
 from ._abi import check, lib
 
-AUTOMATA = {"game-of-life": 0, "wire": 1, "excitable": 2}
+def _registry() -> dict[str, int]:
+    out = {}
+    for i in range(lib.cb2_automaton_count()):
+        name = ctypes.c_char_p()
+        check(lib.cb2_automaton_info(i, ctypes.byref(name), None, None), "automaton info")
+        out[name.value.decode()] = i
+    return out
+
+
+# Every registered automaton by name: the hand-written networks (0-2), then the
+# lowered DSL automata (bundled, examples, "<name>:dsl" twins).
+AUTOMATA = _registry()
 NAMES = {v: k for k, v in AUTOMATA.items()}
 
 
@@ -34,6 +45,15 @@ def automaton_info(automaton) -> tuple[str, int, int]:
     states = ctypes.c_int()
     check(lib.cb2_automaton_info(a, ctypes.byref(name), ctypes.byref(planes), ctypes.byref(states)))
     return name.value.decode(), planes.value, states.value
+
+
+def state_values(automaton) -> list[int]:
+    """State value of each dictionary index (what the reference's checksum sums)."""
+    a = automaton_id(automaton)
+    n = check(lib.cb2_automaton_values(a, None, 0), "automaton values")
+    arr = (ctypes.c_int64 * n)()
+    check(lib.cb2_automaton_values(a, arr, n), "automaton values")
+    return [int(v) for v in arr]
 
 
 def thresholds(probs) -> np.ndarray:
@@ -78,6 +98,7 @@ class HostGrid:
     data: np.ndarray  # uint8 view of the image bytes
 
     def __post_init__(self):
+        self.automaton = automaton_id(self.automaton)  # a name or an id
         need = layout_bytes(self.automaton, self.layout, self.word_bits, self.x_size, self.y_size)
         self.data = np.ascontiguousarray(self.data).view(np.uint8).reshape(-1)
         if self.data.nbytes != need:
@@ -211,6 +232,14 @@ class DeviceGrid:
     @property
     def time_step(self) -> int:
         return int(lib.cb2_grid_time_step(self._h))
+
+    @time_step.setter
+    def time_step(self, t: int) -> None:
+        check(lib.cb2_grid_set_time_step(self._h, t), "set time_step")
+
+    def set_seed(self, seed: int) -> None:
+        """Random seed of stochastic rules (run_params::seed, default 42)."""
+        check(lib.cb2_grid_set_seed(self._h, seed), "set seed")
 
 
 class Batch:

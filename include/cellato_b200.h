@@ -68,6 +68,16 @@ const char* cb2_last_error(void);
 int cb2_automaton_lookup(const char* name);
 /* name, bit-planes P and number of states of automaton `id`. */
 int cb2_automaton_info(int id, const char** name, int* planes, int* states);
+/* Number of registered automata; ids run from 0 to this minus one.  Ids 0-2
+ * (game-of-life, wire, excitable) run hand-written networks; the others are
+ * Cellato DSL automata (the bundled set, src/automata/registry.hpp:1-35, and
+ * "<name>:dsl" twins of the first three) whose type-level AST
+ * (core/ast.hpp) the library lowered to word-wide code at build time. */
+int cb2_automaton_count(void);
+/* State value of each dictionary index of automaton `id` (index_to_state,
+ * memory/state_dictionary.hpp:10-62, as an integer): writes up to `capacity`
+ * values and returns the number of states. */
+int cb2_automaton_values(int id, int64_t* values, int capacity);
 
 /* ---- tuning ------------------------------------------------------------- */
 /* Knobs of one run; 0 in any field means "choose automatically" (autotuned
@@ -95,6 +105,13 @@ typedef struct cb2_tuning {
  * be a multiple of 32.  Launches only; nothing is synchronised. */
 int cb2_run_bit_planes(int automaton, void* const* a, void* const* b, int64_t x_size, int64_t y_size, int64_t steps,
                        const cb2_tuning* tuning, void* stream, int* result_in_b);
+/* The same starting at generation `time_step` (the 0-based time_step the
+ * reference's evaluators read: alternate_algorithms, Margolus blocks and
+ * probability draws depend on it, traversers/cpu/simple.hpp:59-62) with
+ * random seed `seed` (run_params::seed, 42 in cb2_run_bit_planes). */
+int cb2_run_bit_planes_at(int automaton, void* const* a, void* const* b, int64_t x_size, int64_t y_size,
+                          int64_t time_step, int64_t steps, uint64_t seed, const cb2_tuning* tuning, void* stream,
+                          int* result_in_b);
 
 /* Bytes of the static device scratch behind cb2_run_bit_planes_in_place. */
 #define CB2_STATIC_SCRATCH_BYTES (16u << 20)
@@ -140,15 +157,21 @@ int64_t cb2_layout_bytes(int automaton, int layout, int word_bits, int64_t x_siz
 /* Seeded input on the device: cell i = y*x_size + x draws
  * u = SplitMix64(seed + (i+1)*0x9E3779B97F4A7C15) >> 11 and takes state
  * index #{j : thresholds[j] <= u}; thresholds are cumulative probabilities
- * times 2^53 (at most 7). */
+ * times 2^53 (fewer than the automaton's states, at most 31). */
 int cb2_grid_fill_random(cb2_grid* grid, uint64_t seed, const uint64_t* thresholds, int n_thresholds, void* stream);
 
-/* Advances the grid `steps` generations (asynchronous on `stream`). */
+/* Advances the grid `steps` generations (asynchronous on `stream`); the
+ * first is generation cb2_grid_time_step(grid), drawn with the grid's seed. */
 int cb2_grid_run(cb2_grid* grid, int64_t steps, const cb2_tuning* tuning, void* stream);
+/* Random seed of stochastic rules (default 42, run_params::seed). */
+int cb2_grid_set_seed(cb2_grid* grid, uint64_t seed);
+/* Sets the generation counter (the time_step of the next generation). */
+int cb2_grid_set_time_step(cb2_grid* grid, int64_t time_step);
 
 /* 16-number checksum of the current generation
  * (memory/standard_grid.hpp:182-218).  state_values maps dictionary index ->
- * enum value (NULL = identity).  Synchronises `stream`. */
+ * state value (NULL = the automaton's own, cb2_automaton_values).
+ * Synchronises `stream`. */
 int cb2_grid_checksum(cb2_grid* grid, const int64_t* state_values, int n_values, uint64_t out[16], void* stream);
 
 /* Device pointers of the current generation's planes (like grid::data()). */
@@ -248,7 +271,7 @@ typedef struct cb2_request {
     int64_t steps;
     uint64_t seed;          /* seeded input (cb2_grid_fill_random) when host_cells is NULL */
     int n_thresholds;
-    uint64_t thresholds[7];
+    uint64_t thresholds[7];  /* at most 7 (the first 8 states of a larger dictionary) */
     const uint8_t* host_cells; /* optional input, one dictionary index per cell; read at
                                   admission, so it must stay valid until then            */
     uint8_t* host_result;      /* optional output, one index per cell, written at completion */

@@ -78,6 +78,8 @@ def _reflib():
         lib.ref_pack.argtypes = [ctypes.c_int] * 5 + [_u8p, _u8p, ctypes.c_size_t]
         lib.ref_bench.argtypes = [ctypes.c_int] * 7 + [_u8p]
         lib.ref_bench.restype = ctypes.c_double
+        lib.ref_run_seeded.argtypes = [ctypes.c_int] * 7 + [_u8p, _u8p, ctypes.c_char_p, ctypes.c_int]
+        lib.ref_automaton_id.argtypes = [ctypes.c_char_p]
         _ref = lib
     return _ref
 
@@ -191,6 +193,29 @@ def ref_run(automaton: int, cells: np.ndarray, steps: int, layout: str = "standa
     rc = _reflib().ref_run(automaton, LAYOUTS[layout], word_bits, x, y, steps, _p(c, _u8p), _p(out, _u8p), buf, 1024)
     if rc:
         raise ValueError(f"ref_run failed ({rc})")
+    return out, buf.value.decode()
+
+
+def ref_automaton(name: str) -> int:
+    """The reference shim's id of the automaton called `name` (config::name)."""
+    i = _reflib().ref_automaton_id(name.encode())
+    if i < 0:
+        raise KeyError(name)
+    return i
+
+
+def ref_run_named(name: str, cells: np.ndarray, steps: int, seed: int = 42, layout: str = "standard",
+                  word_bits: int = 64):
+    """Reference CPU simple traverser for any automaton the shim knows, with the
+    run's random seed; returns (final cells, checksum string)."""
+    c = np.ascontiguousarray(cells, dtype=np.uint8)
+    y, x = c.shape
+    out = np.empty_like(c)
+    buf = ctypes.create_string_buffer(1024)
+    rc = _reflib().ref_run_seeded(ref_automaton(name), LAYOUTS[layout], word_bits, x, y, steps, seed, _p(c, _u8p),
+                                  _p(out, _u8p), buf, 1024)
+    if rc:
+        raise ValueError(f"ref_run_seeded failed ({rc})")
     return out, buf.value.decode()
 
 

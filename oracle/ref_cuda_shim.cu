@@ -11,7 +11,9 @@
 //   traverser 1: cuda::temporal (traversers/cuda/temporal.cuh:43-245), k
 //                generations per launch in shared-memory tiles
 //
-// both over the reference's linear bit_planes layout with 64-bit words
+// Automaton ids are oracle/ref_shim.cpp's (ref_automaton_id): the bundled
+// set plus the two examples of include/cellato_b200/dsl_examples.hpp.
+// Both traversers run over the reference's linear bit_planes layout with 64-bit words
 // (memory/bit_planes_grid.hpp:35-271), the suites
 // on_cuda::using_<uint64_t>::bit_planes / temporal_linear_bit_planes
 // (experiments/test_suites.hpp:237-258).  Timing follows
@@ -44,9 +46,18 @@ using block_size_y = std::integer_sequence<idx_type, 4, 8, 16>;
 #include "cellato/traversers/cuda/simple.cuh"
 #include "cellato/traversers/cuda/temporal.cuh"
 
+#include "brian/config.hpp"
+#include "critters/config.hpp"
+#include "cyclic/config.hpp"
 #include "excitable/config.hpp"
+#include "fire/config.hpp"
+#include "fluid/config.hpp"
 #include "game_of_life/config.hpp"
+#include "maze/config.hpp"
+#include "traffic/config.hpp"
 #include "wire/config.hpp"
+
+#include "cellato_b200/dsl_examples.hpp"
 
 namespace {
 
@@ -146,6 +157,19 @@ int ref_cuda_run(int automaton, int traverser, int x, int y, int warm_steps, int
         case 2:
             return with_traverser<excitable::config>(traverser, x, y, warm_steps, steps, k, tile_y, block_y,
                                                      planes_in, planes_out, ms);
+#define CB2_REF_CASE(ID, CONFIG)                                                                                       \
+    case ID:                                                                                                           \
+        return with_traverser<CONFIG>(traverser, x, y, warm_steps, steps, k, tile_y, block_y, planes_in, planes_out, ms);
+            CB2_REF_CASE(3, brian::config)
+            CB2_REF_CASE(4, critters::config)
+            CB2_REF_CASE(5, cyclic::config)
+            CB2_REF_CASE(6, fire::config)
+            CB2_REF_CASE(7, fluid::config)
+            CB2_REF_CASE(8, maze::config)
+            CB2_REF_CASE(9, traffic::config)
+            CB2_REF_CASE(10, cellato_b200::examples::forest_fire_config)
+            CB2_REF_CASE(11, cellato_b200::examples::noisy_life_config)
+#undef CB2_REF_CASE
         default: put_error(err, errlen, "unknown automaton"); return -1;
         }
     } catch (const std::exception& e) {

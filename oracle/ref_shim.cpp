@@ -24,9 +24,18 @@
 #include "cellato/experiments/run_params.hpp"
 #include "cellato/experiments/test_suites.hpp"
 
+#include "brian/config.hpp"
+#include "critters/config.hpp"
+#include "cyclic/config.hpp"
 #include "excitable/config.hpp"
+#include "fire/config.hpp"
+#include "fluid/config.hpp"
 #include "game_of_life/config.hpp"
+#include "maze/config.hpp"
+#include "traffic/config.hpp"
 #include "wire/config.hpp"
+
+#include "cellato_b200/dsl_examples.hpp"
 
 namespace {
 
@@ -35,7 +44,8 @@ namespace ts = cellato::run::test_suites;
 enum layout_id { L_STANDARD = 0, L_BIT_ARRAY = 1, L_BIT_PLANES = 2, L_TILED = 3 };
 
 template <typename suite>
-int run_suite(int x, int y, int steps, const uint8_t* in, uint8_t* out, char* checksum, int checksum_len) {
+int run_suite(int x, int y, int steps, const uint8_t* in, uint8_t* out, char* checksum, int checksum_len,
+              int seed = 42) {
     using automaton = typename suite::automaton;
     using dict = typename automaton::state_dictionary;
     using cell_t = typename suite::original_cell_t;
@@ -46,6 +56,7 @@ int run_suite(int x, int y, int steps, const uint8_t* in, uint8_t* out, char* ch
     params.x_size = x;
     params.y_size = y;
     params.steps = steps;
+    params.seed = seed;
 
     cellato::memory::grids::standard::grid<cell_t> initial(x, y);
     cell_t* data = initial.data();
@@ -98,6 +109,15 @@ int with_automaton(int automaton, int layout, int word_bits, fn_t&& fn) {
     case 0: return with_suite<game_of_life::config>(layout, word_bits, fn);
     case 1: return with_suite<wire::config>(layout, word_bits, fn);
     case 2: return with_suite<excitable::config>(layout, word_bits, fn);
+    case 3: return with_suite<brian::config>(layout, word_bits, fn);
+    case 4: return with_suite<critters::config>(layout, word_bits, fn);
+    case 5: return with_suite<cyclic::config>(layout, word_bits, fn);
+    case 6: return with_suite<fire::config>(layout, word_bits, fn);
+    case 7: return with_suite<fluid::config>(layout, word_bits, fn);
+    case 8: return with_suite<maze::config>(layout, word_bits, fn);
+    case 9: return with_suite<traffic::config>(layout, word_bits, fn);
+    case 10: return with_suite<cellato_b200::examples::forest_fire_config>(layout, word_bits, fn);
+    case 11: return with_suite<cellato_b200::examples::noisy_life_config>(layout, word_bits, fn);
     default: return -1;
     }
 }
@@ -153,6 +173,27 @@ int ref_run(int automaton, int layout, int word_bits, int x, int y, int steps, c
     } catch (...) {
         return -10;
     }
+}
+
+// ref_run with the run's random seed (run_params::seed; 42 in ref_run).
+int ref_run_seeded(int automaton, int layout, int word_bits, int x, int y, int steps, int seed, const uint8_t* in,
+                   uint8_t* out, char* checksum, int checksum_len) {
+    try {
+        return with_automaton(automaton, layout, word_bits, [&]<typename suite>() {
+            return run_suite<suite>(x, y, steps, in, out, checksum, checksum_len, seed);
+        });
+    } catch (...) {
+        return -10;
+    }
+}
+
+// The shim's automaton ids by the reference's names (config::name), -1 if unknown.
+int ref_automaton_id(const char* name) {
+    static const char* const names[] = {"game-of-life", "wire",  "excitable", "brian",   "critters",         "cyclic",
+                                        "forest-fire",  "fluid", "maze",      "traffic", "lightning-forest", "noisy-life"};
+    for (int i = 0; i < (int)(sizeof(names) / sizeof(names[0])); ++i)
+        if (name && std::strcmp(name, names[i]) == 0) return i;
+    return -1;
 }
 
 // Host byte image of the layout's grid words (bit_array, bit_planes, tiled).

@@ -55,7 +55,8 @@ def test_grid_create_rejects_bad_sizes_without_touching_the_gpu():
     h = ctypes.c_void_p()
     assert _abi.lib.cb2_grid_create(0, 48, 16, ctypes.byref(h)) == _abi.CB2_EINVAL
     assert "multiple of 32" in _abi.last_error()
-    assert _abi.lib.cb2_grid_create(7, 64, 16, ctypes.byref(h)) == _abi.CB2_ENOTFOUND
+    unknown = _abi.lib.cb2_automaton_count()
+    assert _abi.lib.cb2_grid_create(unknown, 64, 16, ctypes.byref(h)) == _abi.CB2_ENOTFOUND
 
 
 def test_tuning_file_round_trip(tmp_path):

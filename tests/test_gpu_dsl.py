@@ -1,0 +1,169 @@
+"""The lowered DSL path (cb2_ast.cuh): every bundled Cellato automaton and the
+two user-defined examples, advanced by the strip kernels and compared cell
+for cell with the reference's own CPU traverser (oracle/_ref, standard
+layout) on the same input -- including the stochastic rules, whose draws
+must reproduce the reference's counter-based stream.  The ":dsl" twins of
+the hand-written networks must agree with those networks."""
+import random
+
+import numpy as np
+import pytest
+
+import cellato_b200 as cb
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+DSL = ["brian", "critters", "cyclic", "forest-fire", "fluid", "maze", "traffic", "lightning-forest", "noisy-life"]
+PROBS = {"traffic": [0.6, 0.2, 0.2], "lightning-forest": [0.3, 0.6, 0.1], "noisy-life": [0.6, 0.4],
+         "maze": [0.7, 0.3], "critters": [0.5, 0.5], "brian": [0.5, 0.2, 0.3]}
+
+
+@pytest.fixture(scope="module")
+def ref(cuda):
+    if not O.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    missing = [n for n in DSL if n not in cb.AUTOMATA]
+    if missing:
+        pytest.fail(f"library built without the lowered DSL automata: {missing}")
+    return O
+
+
+def cells_for(name, x, y, seed):
+    _, _, states = cb.automaton_info(name)
+    probs = PROBS.get(name, [1.0 / states] * states)
+    return O.init_cells(x, y, seed, O.thresholds(probs))
+
+
+def device_run(name, cells, steps, seed=42, time_step=0, **plan):
+    y, x = cells.shape
+    with cb.DeviceGrid(name, x, y) as g:
+        g.upload_cells(cells)
+        g.set_seed(seed)
+        g.time_step = time_step
+        g.run(steps, **plan)
+        return g.cells(), g.checksum_str()
+
+
+@pytest.mark.parametrize("name", DSL)
+def test_default_plan_matches_the_reference(ref, name):
+    for (x, y, steps, seed) in [(64, 48, 37, 1), (32 * 37, 61, 20, 2), (96, 7, 9, 3)]:
+        cells = cells_for(name, x, y, seed)
+        want, want_ck = ref.ref_run_named(name, cells, steps)
+        got, ck = device_run(name, cells, steps)
+        assert (got == want).all(), (name, x, y, steps)
+        assert ck == want_ck, (name, x, y, steps)
+
+
+@pytest.mark.parametrize("name", DSL)
+def test_every_lowered_variant_matches_the_reference(ref, name):
+    x, y, steps = 32 * 70, 37, 21  # 2+ strips wide with a ragged last strip, odd height
+    cells = cells_for(name, x, y, 11)
+    want, _ = ref.ref_run_named(name, cells, steps)
+    for (k, v, lv, r) in cb.variants(name):
+        got, _ = device_run(name, cells, steps, temporal_steps=k, words_per_lane=v, levels_per_warp=lv,
+                            rows_per_step=r, tile_rows=9)
+        assert (got == want).all(), (name, k, v, lv, r)
+
+
+@pytest.mark.parametrize("name", ["lightning-forest", "noisy-life", "critters", "traffic"])
+def test_time_and_seed_dependent_rules(ref, name):
+    x, y = 256, 65
+    cells = cells_for(name, x, y, 5)
+    for seed in (42, 7, 123456789):
+        want, _ = ref.ref_run_named(name, cells, 33, seed=seed)
+        got, _ = device_run(name, cells, 33, seed=seed)
+        assert (got == want).all(), (name, seed)
+    # generations counted across runs: 12 then 21 more equal one run of 33
+    want, _ = ref.ref_run_named(name, cells, 33)
+    with cb.DeviceGrid(name, x, y) as g:
+        g.upload_cells(cells)
+        g.run(12)
+        g.run(21)
+        assert g.time_step == 33
+        assert (g.cells() == want).all()
+
+
+def test_random_shapes_and_plans(ref):
+    rng = random.Random(77)
+    for trial in range(40):
+        name = rng.choice(DSL)
+        x = 32 * rng.choice([1, 2, 3, 31, 32, 33, 64])
+        y = rng.choice([1, 2, 3, 8, 17, 40])
+        steps = rng.randrange(0, 30)
+        k, v, lv, r = rng.choice(cb.variants(name))
+        cells = cells_for(name, x, y, trial)
+        want, _ = ref.ref_run_named(name, cells, steps)
+        got, _ = device_run(name, cells, steps, temporal_steps=k, words_per_lane=v, levels_per_warp=lv,
+                            rows_per_step=r, tile_rows=rng.choice([0, 1, 5, 100]))
+        assert (got == want).all(), (trial, name, x, y, steps, (k, v, lv, r))
+
+
+@pytest.mark.parametrize("base", ["game-of-life", "wire", "excitable"])
+def test_dsl_twins_equal_the_hand_written_networks(cuda, base):
+    x, y, steps = 2048, 1024, 100
+    _, _, states = cb.automaton_info(base)
+    cells = O.init_cells(x, y, 3, O.thresholds([1.0 / states] * states))
+    hand, hand_ck = device_run(base, cells, steps)
+    dsl, dsl_ck = device_run(base + ":dsl", cells, steps)
+    assert (hand == dsl).all()
+    assert hand_ck == dsl_ck
+
+
+def test_checksum_sums_state_values_not_indexes(ref):
+    # forest-fire's dictionary lists (empty, tree, fire, ash) but the enum is
+    # (empty, tree, ash, fire): the checksum must sum the enum values
+    assert cb.grid.state_values("forest-fire") == [0, 1, 3, 2]
+    cells = cells_for("forest-fire", 128, 64, 9)
+    want, want_ck = ref.ref_run_named("forest-fire", cells, 15)
+    _, ck = device_run("forest-fire", cells, 15)
+    assert ck == want_ck
+
+
+def test_dsl_automata_outside_the_strip_kernels_are_refused(cuda):
+    with cb.DeviceGrid("brian", 64, 64) as g:
+        with pytest.raises(ValueError, match="batch kernel runs"):
+            cb.Batch([g], [10])
+    from cellato_b200 import _abi
+    from cellato_b200.bands import BandGrid, _planes
+    import ctypes
+    b = BandGrid("game-of-life", 256, 64)
+    t = _abi.tuning()
+    rc = _abi.lib.cb2_band_pass(cb.AUTOMATA["brian"], _planes(b.bufs[0]), _planes(b.bufs[1]), 256, b.rows_total,
+                                b.ghost, 64, 4, ctypes.byref(t), None)
+    assert rc == _abi.CB2_EINVAL and "hand-written networks" in _abi.last_error()
+
+
+def test_served_dsl_requests(ref):
+    mix = [("cyclic", 96, 40, 17, 1), ("lightning-forest", 64, 64, 25, 2), ("critters", 128, 33, 12, 3),
+           ("game-of-life", 64, 64, 30, 4), ("traffic", 96, 48, 40, 5)]
+    with cb.Server(chunk_steps=8) as srv:
+        jobs = []
+        for (name, x, y, steps, seed) in mix:
+            cells = cells_for(name, x, y, seed)
+            jobs.append((name, cells, steps, seed, srv.submit(name, x, y, steps, cells=cells, want_cells=True)))
+        srv.drain(120)
+        for name, cells, steps, seed, rid in jobs:
+            assert srv.wait(rid)["state"] == "done"
+            # a request's random seed is its seed field (0 when it brings its own cells)
+            want, _ = ref.ref_run_named(name, cells, steps, seed=0)
+            assert (srv.result_cells(rid) == want).all(), name
+
+
+def test_golden_fixtures(cuda):
+    # committed outputs of the reference traverser: independent of oracle/_ref
+    import json
+    import os
+    here = os.path.join(os.path.dirname(__file__), "golden")
+    with open(os.path.join(here, "golden_dsl.json")) as f:
+        cases = json.load(f)["cases"]
+    arrays = np.load(os.path.join(here, "golden_dsl.npz"))
+    for c in cases:
+        thr = np.array(c["thresholds"], dtype=np.uint64)
+        with cb.DeviceGrid(c["automaton"], c["x"], c["y"]) as g:
+            g.fill_random(c["input_seed"], thr=thr)
+            g.set_seed(c["seed"])
+            g.run(c["steps"])
+            assert g.checksum_str() == c["checksum"], c
+            if "cells" in c:
+                assert (g.cells() == arrays[c["cells"] + "_out"]).all(), c
