@@ -204,10 +204,16 @@ __device__ __forceinline__ uint32_t bernoulli_word(const cell_ctx& c, uint64_t s
             return dyadic_draw<n, d>(s);
         } else {
             // Recurring expansion: draw until every lane has left the threshold.
+            // The stream is counter-based, so the first kAhead draws are computed
+            // up front as independent instructions and consumed in order; draws
+            // past the one that resolves the last lane are simply not used.
+            constexpr int kAhead = 8;
+            uint32_t ahead[kAhead];
+#pragma unroll
+            for (int j = 0; j < kAhead; ++j) ahead[j] = s.next();
             uint32_t active = 0xffffffffu, result = 0;
             uint64_t rem = n;
-            while (active) {
-                const uint32_t bits = s.next();
+            auto digit = [&](uint32_t bits) {
                 if (rem >= d - rem) {
                     rem -= d - rem;
                     result |= active & ~bits;
@@ -216,7 +222,11 @@ __device__ __forceinline__ uint32_t bernoulli_word(const cell_ctx& c, uint64_t s
                     rem += rem;
                     active &= ~bits;
                 }
-            }
+            };
+#pragma unroll
+            for (int j = 0; j < kAhead; ++j)
+                if (active) digit(ahead[j]);
+            while (active) digit(s.next());
             return result;
         }
     }

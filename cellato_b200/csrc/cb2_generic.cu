@@ -10,6 +10,12 @@
 // cb2_launch.cuh run it: pipe_run_rows with a window of 3P words per row,
 // one or two words per lane, a few levels per warp.
 //
+// A user's own automata join the table at build time: a header that defines
+// their configs and the list macro CB2_USER_CONFIGS(X), e.g.
+//     #define CB2_USER_CONFIGS(X) X(my_rules::config) X(other::config)
+// named by `make USER_AUTOMATA=path/to/rules.hpp` (csrc/Makefile), is
+// included here and each listed config is registered under its name.
+//
 // Built only when the Cellato headers are present (csrc/Makefile, CELLATO);
 // cb2_generic_none.cpp stands in otherwise and registers nothing.
 #include <cuda_runtime.h>
@@ -33,6 +39,10 @@
 #include "wire/config.hpp"
 
 #include "cellato_b200/dsl_examples.hpp"
+
+#ifdef CB2_USER_AUTOMATA
+#include CB2_USER_AUTOMATA
+#endif
 
 namespace cb2 {
 namespace {
@@ -95,6 +105,11 @@ const dsl_table& table() {
         add<::game_of_life::config>(d, "game-of-life:dsl");
         add<::wire::config>(d, "wire:dsl");
         add<::excitable::config>(d, "excitable:dsl");
+#ifdef CB2_USER_CONFIGS
+#define CB2_ADD_USER_CONFIG(C) add<C>(d, C::name);
+        CB2_USER_CONFIGS(CB2_ADD_USER_CONFIG)
+#undef CB2_ADD_USER_CONFIG
+#endif
         return d;
     }();
     return t;

@@ -184,6 +184,8 @@ public:
         cb2_grid* g = nullptr;
         check(cb2_grid_create(id, _x, _y, &g), "cb2_grid_create");
         _grid.reset(g);
+        // stochastic rules draw with the run's seed (traversers/cpu/simple.hpp:30)
+        check(cb2_grid_set_seed(_grid.get(), static_cast<uint64_t>(params.seed)), "cb2_grid_set_seed");
         std::vector<uint8_t> img;
         layout::save(grid, img);
         check(cb2_grid_upload(_grid.get(), layout::layout, layout::word_bits, img.data(), img.size(), nullptr),
