@@ -115,6 +115,8 @@ _SIGNATURES = {
                                              _vp, ctypes.POINTER(ctypes.c_int)]),
     "cb2_run_bit_planes_in_place": (ctypes.c_int, [ctypes.c_int, _vpp, _i64, _i64, _i64, _tp, _vp]),
     "cb2_band_pass": (ctypes.c_int, [ctypes.c_int, _vpp, _vpp, _i64, _i64, _i64, _i64, ctypes.c_int, _tp, _vp]),
+    "cb2_band_pass_at": (ctypes.c_int, [ctypes.c_int, _vpp, _vpp, _i64, _i64, _i64, _i64, ctypes.c_int, _i64,
+                                        ctypes.c_uint64, _i64, _i64, _tp, _vp]),
     "cb2_fill_random_planes": (ctypes.c_int, [ctypes.c_int, _vpp, _i64, _i64, _i64, _i64, ctypes.c_uint64, _u64p,
                                               ctypes.c_int, _vp]),
     "cb2_checksum_planes": (ctypes.c_int, [ctypes.c_int, _vpp, _i64, _i64, _i64, _i64, _i64, _i64, _i64p,

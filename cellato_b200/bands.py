@@ -17,6 +17,7 @@ run reproduces the single-grid run cell for cell.
 from __future__ import annotations
 
 import ctypes
+from fractions import Fraction
 
 import torch
 import torch.distributed as dist
@@ -84,13 +85,14 @@ class BandGrid:
         self.bufs = [torch.zeros(shape, dtype=torch.int32, device=self.device) for _ in range(2)]
         self.cur = 0
         self.time_step = 0
+        self.seed = 42  # random seed of stochastic rules (run_params::seed)
 
     @property
     def planes(self) -> torch.Tensor:
         return self.bufs[self.cur]
 
     def fill_random(self, seed: int, probs=None, stream=None) -> None:
-        thr = thresholds(probs if probs is not None else [1.0 / self.states] * self.states)
+        thr = thresholds(probs if probs is not None else [Fraction(1, self.states)] * self.states)
         arr = (ctypes.c_uint64 * max(1, len(thr)))(*[int(v) for v in thr])
         check(lib.cb2_fill_random_planes(self.automaton, _planes(self.planes), self.x_size, self.rows_total,
                                          self.row0 - self.ghost, self.global_rows, seed, arr, len(thr),
@@ -111,9 +113,11 @@ class BandGrid:
             while k > left:
                 k //= 2
             exchange_halos(self.planes, self.ghost, self.band, k, self.rank, self.world, self.group)
-            check(lib.cb2_band_pass(self.automaton, _planes(self.bufs[self.cur]), _planes(self.bufs[1 - self.cur]),
-                                    self.x_size, self.rows_total, self.ghost, self.band, k, ctypes.byref(t),
-                                    _stream(stream)), "band pass")
+            check(lib.cb2_band_pass_at(self.automaton, _planes(self.bufs[self.cur]),
+                                       _planes(self.bufs[1 - self.cur]), self.x_size, self.rows_total, self.ghost,
+                                       self.band, k, self.time_step + (steps - left), self.seed,
+                                       self.row0 - self.ghost, self.global_rows, ctypes.byref(t), _stream(stream)),
+                  "band pass")
             self.cur ^= 1
             left -= k
             passes += 1

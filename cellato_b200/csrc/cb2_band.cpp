@@ -47,13 +47,24 @@ extern "C" {
 
 int cb2_band_pass(int automaton, void* const* in, void* const* out, int64_t x_size, int64_t rows_total,
                   int64_t row_first, int64_t rows_out, int temporal_steps, const cb2_tuning* tuning, void* stream) {
+    if (automaton >= kNumBuiltin && automaton < automaton_count()) {
+        // A lowered DSL rule may read the cells' generation and global row
+        // (Margolus blocks, probability draws), which only cb2_band_pass_at knows.
+        set_error("a lowered DSL automaton needs the band's global rows and generation: use cb2_band_pass_at");
+        return CB2_EINVAL;
+    }
+    return cb2_band_pass_at(automaton, in, out, x_size, rows_total, row_first, rows_out, temporal_steps, 0,
+                            kDefaultSeed, 0, rows_total, tuning, stream);
+}
+
+int cb2_band_pass_at(int automaton, void* const* in, void* const* out, int64_t x_size, int64_t rows_total,
+                     int64_t row_first, int64_t rows_out, int temporal_steps, int64_t time_step, uint64_t seed,
+                     int64_t global_row0, int64_t global_rows, const cb2_tuning* tuning, void* stream) {
     grid_geom g;
     int rc = make_geom(automaton, x_size, rows_total, &g);
     if (rc) return rc;
-    if (automaton >= kNumBuiltin) {
-        // A lowered DSL rule may read the cells' global row (Margolus blocks,
-        // probability draws); a band pass only knows band-local rows.
-        set_error("row bands run the hand-written networks (game-of-life, wire, excitable) only");
+    if (time_step < 0 || global_rows < 1) {
+        set_error("negative time_step or empty global grid");
         return CB2_EINVAL;
     }
     if ((rc = check_planes(g, in, "input")) || (rc = check_planes(g, out, "output"))) return rc;
@@ -77,8 +88,10 @@ int cb2_band_pass(int automaton, void* const* in, void* const* out, int64_t x_si
     run_plan plan;
     rc = resolve_plan(window, &t, &plan);
     if (rc) return rc;
+    int64_t row0 = global_row0 % global_rows;  // the planes' row 0 (a ghost row for rank 0) as a global row
+    if (row0 < 0) row0 += global_rows;
     cudaError_t e = launch_strip_window(g, (const uint32_t*)in[0], (uint32_t*)out[0], plan, (int)row_first,
-                                        (int)rows_out, (cudaStream_t)stream);
+                                        (int)rows_out, (cudaStream_t)stream, time_step, seed, row0, global_rows);
     if (e != cudaSuccess) return cuda_err(e, "band pass launch");
     return CB2_OK;
 }
@@ -109,8 +122,12 @@ int cb2_checksum_planes(int automaton, const void* const* planes, int64_t x_size
     if (rc) return rc;
     if ((rc = check_planes(g, planes, "input"))) return rc;
     if (!out || n_values < 0 || n_values > (1 << kMaxPlanes) || (n_values && !values)) {
-        set_error("null output or more than 8 state values");
+        set_error("null output or more than " + std::to_string(1 << kMaxPlanes) + " state values");
         return CB2_EINVAL;
+    }
+    if (!values) {  // the dictionary's own state values, as the reference's standard grid sums them
+        values = automaton_at(automaton)->values;
+        n_values = automaton_at(automaton)->states;
     }
     if (row_first < 0 || row_count < 0 || row_first + row_count > rows || global_row0 < 0 ||
         global_row0 + row_count > global_rows) {
@@ -122,8 +139,8 @@ int cb2_checksum_planes(int automaton, const void* const* planes, int64_t x_size
     cudaError_t e = cudaMallocAsync(&sums, 16 * sizeof(unsigned long long), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(sums, 0, 16 * sizeof(unsigned long long), s);
     if (e == cudaSuccess)
-        e = launch_checksum_rows(g, (const uint32_t*)planes[0], values, values ? n_values : 0, row_first, row_count,
-                                 global_row0, global_rows, sums, s);
+        e = launch_checksum_rows(g, (const uint32_t*)planes[0], values, n_values, row_first, row_count, global_row0,
+                                 global_rows, sums, s);
     unsigned long long host[16] = {};
     if (e == cudaSuccess) e = cudaMemcpyAsync(host, sums, sizeof(host), cudaMemcpyDeviceToHost, s);
     if (sums) cudaFreeAsync(sums, s);

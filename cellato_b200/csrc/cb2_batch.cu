@@ -116,6 +116,10 @@ __global__ void __launch_bounds__(kBatchWarps * 32) batch_kernel(batch_args a) {
         st.in = gd.buf[task.chunk & 1];
         st.out = gd.buf[(task.chunk & 1) ^ 1];
         st.plane_words = gd.plane_words;
+        st.t0 = 0;  // the hand-written networks read neither time, seed nor global rows
+        st.seed = 0;
+        st.y_global0 = 0;
+        st.global_h = gd.h;
         st.wd = gd.wd;
         st.h = gd.h;
         lane_geom<1> geom;

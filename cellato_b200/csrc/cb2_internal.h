@@ -68,9 +68,11 @@ const automaton_desc* generic_desc(int i);
 cudaError_t launch_strip_pass(const grid_geom& g, const uint32_t* in, uint32_t* out, const run_plan& plan,
                               cudaStream_t stream, int64_t t0 = 0, uint64_t seed = kDefaultSeed);
 // The same for output rows [y_base, y_base + rows_out) only (input rows wrap mod g.h).
+// y_global0 / global_h place the planes' rows in a larger grid (a band of
+// it): rules that read the row see global rows (0 = the planes are the grid).
 cudaError_t launch_strip_window(const grid_geom& g, const uint32_t* in, uint32_t* out, const run_plan& plan,
                                 int y_base, int rows_out, cudaStream_t stream, int64_t t0 = 0,
-                                uint64_t seed = kDefaultSeed);
+                                uint64_t seed = kDefaultSeed, int64_t y_global0 = 0, int64_t global_h = 0);
 // Strip tasks per column and per row for a plan.
 void strip_counts(const grid_geom& g, int v, int tile_rows, int* nsx, int* nsy);
 // The instantiated kernels of an automaton, and the first one matching a

@@ -108,7 +108,8 @@ int auto_tile_rows(const grid_geom& g, const strip_variant& sv) {
 }
 
 cudaError_t launch_strip_window(const grid_geom& g, const uint32_t* in, uint32_t* out, const run_plan& plan,
-                                int y_base, int rows_out, cudaStream_t stream, int64_t t0, uint64_t seed) {
+                                int y_base, int rows_out, cudaStream_t stream, int64_t t0, uint64_t seed,
+                                int64_t y_global0, int64_t global_h) {
     const strip_variant* sv = find_variant(g.automaton, plan.k, plan.v, plan.l, plan.r);
     if (!sv || rows_out < 1 || y_base < 0 || y_base + rows_out > g.h) return cudaErrorInvalidValue;
     resident_strip_tasks(*sv);  // sets the kernel's shared-memory attribute once
@@ -123,6 +124,8 @@ cudaError_t launch_strip_window(const grid_geom& g, const uint32_t* in, uint32_t
     a.rows_out = rows_out;
     a.t0 = t0;
     a.seed = seed;
+    a.y_global0 = y_global0;
+    a.global_h = global_h > 0 ? global_h : g.h;
     grid_geom window = g;
     window.h = rows_out;
     strip_counts(window, plan.v, plan.tile_rows, &a.nsx, &a.nsy);

@@ -23,6 +23,8 @@ struct strip_launch {
     int32_t y_base, rows_out;  // output rows [y_base, y_base + rows_out)
     int64_t t0;                // generation of the input
     uint64_t seed;             // random seed of stochastic rules
+    int64_t y_global0;         // global row of row 0 of the planes (a band's offset)
+    int64_t global_h;          // rows of the whole grid
 };
 
 template <class R, int K, int V, int L, int RPS>
@@ -43,6 +45,8 @@ __global__ void __launch_bounds__(32 * (K / L)) pipe_kernel(strip_launch a) {
     t.ny = min(a.tile_rows, a.y_base + a.rows_out - t.y0);
     t.t0 = a.t0;
     t.seed = a.seed;
+    t.y_global0 = a.y_global0;
+    t.global_h = a.global_h;
     if constexpr (RPS > 1)
         pipe_run_rows<R, K, V, L, kRingDepth, RPS>(t, smem);  // RPS rows per barrier
     else if constexpr (L == K)

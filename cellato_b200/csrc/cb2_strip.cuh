@@ -43,6 +43,8 @@ struct strip_task {
     int32_t y0, ny;       // first output row, output row count (1 .. h - y0)
     int64_t t0;           // generation of the input (read by rules that depend on time)
     uint64_t seed;        // random seed of the run (read by stochastic rules)
+    int64_t y_global0;    // global row of row 0 of these planes (a band's offset; 0 for a whole grid)
+    int64_t global_h;     // rows of the whole grid (h for a whole grid)
 };
 
 // Where a lane's 32 cells are, for rules that read it (window rules): the
@@ -61,9 +63,11 @@ struct cell_ctx {
 struct row_ctx {
     int64_t t;     // generation of the first level of the chain
     int sweep;     // sweep index of the row entering the first level
-    int y_base;    // grid row of sweep index 0 (y0 - K)
-    int h;         // rows of the grid
+    int y_base;    // row of sweep index 0 in these planes (y0 - K)
+    int h;         // rows of these planes
     uint64_t seed;
+    int64_t y_global0;  // global row of row 0 of these planes
+    int64_t global_h;   // rows of the whole grid
 };
 
 constexpr unsigned kFullMask = 0xffffffffu;
@@ -153,6 +157,7 @@ __device__ __forceinline__ void level_push(strip_state<R, K, V>& s, int g, uint3
         // level g outputs the row one above its input: sweep index rc->sweep - g - 1
         int64_t y = ((int64_t)rc->y_base + rc->sweep - g - 1) % rc->h;
         if (y < 0) y += rc->h;
+        y = (y + rc->y_global0) % rc->global_h;  // a band's rows are global rows y_global0..
         uint32_t nxt[V][P];
 #pragma unroll
         for (int i = 0; i < V; ++i) {

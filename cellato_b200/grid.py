@@ -64,8 +64,8 @@ def thresholds(probs) -> np.ndarray:
     reproducible on any host.
     """
     fr = [p if isinstance(p, Fraction) else Fraction(str(p)) for p in probs]
-    if sum(fr) != 1:
-        raise ValueError(f"probabilities sum to {sum(fr)}, not 1")
+    if abs(sum(fr) - 1) > Fraction(1, 10**12):  # decimal floats such as 1/3 sum to 1 only within rounding
+        raise ValueError(f"probabilities sum to {float(sum(fr))}, not 1")
     out, cum = [], Fraction(0)
     for p in fr[:-1]:
         cum += p
@@ -199,6 +199,8 @@ class DeviceGrid:
 
     def fill_random(self, seed: int, probs=None, thr: np.ndarray | None = None, stream=None) -> None:
         if thr is None:
+            if probs is None:  # uniform over the dictionary
+                probs = [Fraction(1, self.states)] * self.states
             thr = thresholds(probs)
         t = np.ascontiguousarray(thr, dtype=np.uint64)
         check(lib.cb2_grid_fill_random(self._h, seed, t.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), len(t),

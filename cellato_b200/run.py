@@ -18,6 +18,7 @@ from __future__ import annotations
 import argparse
 import math
 import sys
+from fractions import Fraction
 
 from . import grid as G
 from .traverser import RunParams
@@ -84,13 +85,14 @@ def main(argv=None) -> int:
     import torch
 
     name, planes, states = G.automaton_info(a.automaton)
-    probs = a.density or [1.0 / states] * states
+    probs = a.density or [Fraction(1, states)] * states
     thr = G.thresholds(probs)
     stream = torch.cuda.current_stream()
     times, checksums = [], []
     for r in range(a.warmup_rounds + a.rounds):
         with G.DeviceGrid(a.automaton, a.x_size, a.y_size) as g:
             g.fill_random(a.seed, thr=thr, stream=stream)
+            g.set_seed(a.seed)  # the run's random seed, as run_params::seed is for the reference
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             g.run(a.steps, a.temporal_steps, a.temporal_tile_size_y, a.words_per_lane, a.levels_per_warp,

@@ -3,6 +3,7 @@ simulation requests with admission by device-memory budget."""
 from __future__ import annotations
 
 import ctypes
+from fractions import Fraction
 
 import numpy as np
 
@@ -61,7 +62,8 @@ class Server:
             req.host_cells = c.ctypes.data
         else:
             if probs is None:
-                probs = [1.0 / automaton_info(a)[2]] * automaton_info(a)[2]
+                states = automaton_info(a)[2]
+                probs = [Fraction(1, states)] * states
             t = thresholds(probs)
             req.n_thresholds = len(t)
             for i, v in enumerate(t):

@@ -191,6 +191,14 @@ int64_t cb2_grid_time_step(const cb2_grid* grid);
  * multi-GPU split of that run. */
 int cb2_band_pass(int automaton, void* const* in, void* const* out, int64_t x_size, int64_t rows_total,
                   int64_t row_first, int64_t rows_out, int temporal_steps, const cb2_tuning* tuning, void* stream);
+/* cb2_band_pass at generation `time_step` with random seed `seed`, for a
+ * band whose planes' row 0 is global row `global_row0` (mod global_rows, so a
+ * rank-0 band with ghost rows passes -ghost) of a grid `global_rows` tall.
+ * Lowered DSL automata need these (Margolus blocks and probability draws read
+ * the generation and the global row); cb2_band_pass refuses them. */
+int cb2_band_pass_at(int automaton, void* const* in, void* const* out, int64_t x_size, int64_t rows_total,
+                     int64_t row_first, int64_t rows_out, int temporal_steps, int64_t time_step, uint64_t seed,
+                     int64_t global_row0, int64_t global_rows, const cb2_tuning* tuning, void* stream);
 /* Seeded input (cb2_grid_fill_random's stream) for caller-owned planes whose
  * row y is global row (global_row0 + y) mod global_rows of the global grid. */
 int cb2_fill_random_planes(int automaton, void* const* planes, int64_t x_size, int64_t rows, int64_t global_row0,

@@ -93,8 +93,8 @@ def thresholds(probs) -> np.ndarray:
     """Cumulative state probabilities (dictionary-index order) as exact 53-bit integer thresholds."""
     fr = [Fraction(str(p)) if not isinstance(p, Fraction) else p for p in probs]
     total = sum(fr)
-    if total != 1:
-        raise ValueError(f"probabilities sum to {total}, not 1")
+    if abs(total - 1) > Fraction(1, 10**12):  # decimal floats such as 1/3 sum to 1 only within rounding
+        raise ValueError(f"probabilities sum to {float(total)}, not 1")
     out, cum = [], Fraction(0)
     for p in fr[:-1]:
         cum += p

@@ -127,11 +127,11 @@ def test_dsl_automata_outside_the_strip_kernels_are_refused(cuda):
     from cellato_b200 import _abi
     from cellato_b200.bands import BandGrid, _planes
     import ctypes
-    b = BandGrid("game-of-life", 256, 64)
+    b = BandGrid("brian", 256, 64)
     t = _abi.tuning()
-    rc = _abi.lib.cb2_band_pass(cb.AUTOMATA["brian"], _planes(b.bufs[0]), _planes(b.bufs[1]), 256, b.rows_total,
+    rc = _abi.lib.cb2_band_pass(b.automaton, _planes(b.bufs[0]), _planes(b.bufs[1]), 256, b.rows_total,
                                 b.ghost, 64, 4, ctypes.byref(t), None)
-    assert rc == _abi.CB2_EINVAL and "hand-written networks" in _abi.last_error()
+    assert rc == _abi.CB2_EINVAL and "cb2_band_pass_at" in _abi.last_error()
 
 
 def test_served_dsl_requests(ref):
@@ -167,3 +167,74 @@ def test_golden_fixtures(cuda):
             assert g.checksum_str() == c["checksum"], c
             if "cells" in c:
                 assert (g.cells() == arrays[c["cells"] + "_out"]).all(), c
+
+
+@pytest.mark.parametrize("name,states", [("brian", 3), ("lightning-forest", 3), ("cyclic", 32)])
+def test_cli_runs_dsl_automata(ref, capsys, name, states):
+    # the reference-style CLI: device-seeded input (uniform states), the run's seed for the draws
+    from fractions import Fraction
+    from cellato_b200 import run
+    x, y, steps, seed = 128, 40, 21, 17
+    assert run.main(["--automaton", name, "--device", "CUDA", "--traverser", "b200", "--x_size", str(x),
+                     "--y_size", str(y), "--steps", str(steps), "--seed", str(seed)]) == 0
+    line = capsys.readouterr().out.strip().splitlines()[-1]
+    cells = O.init_cells(x, y, seed, O.thresholds([Fraction(1, states)] * states))
+    _, want_ck = ref.ref_run_named(name, cells, steps, seed=seed)
+    assert line.endswith("," + want_ck), line
+
+
+@pytest.mark.parametrize("name", ["critters", "lightning-forest", "traffic", "cyclic"])
+def test_two_bands_equal_the_global_grid(ref, name):
+    # Rank r of 2 owns rows [r*B, (r+1)*B); ghost rows are refreshed from the other
+    # band before each pass, as exchange_halos does between GPUs.  Margolus blocks
+    # and probability draws read global rows and generations across the split.
+    import ctypes
+    from cellato_b200 import _abi
+    from cellato_b200.bands import BandGrid, _planes
+    x, rows, steps, seed = 512, 96, 37, 5
+    bands = [BandGrid(name, x, rows, rank=r, world=2) for r in range(2)]
+    for b in bands:
+        b.fill_random(seed, [0.5, 0.25, 0.25] if b.states == 3 else None)
+        b.seed = 9
+    g, B = bands[0].ghost, bands[0].band
+    t = _abi.tuning()
+    left, done = steps, 0
+    while left > 0:
+        k = bands[0].plan_k()
+        while k > left:
+            k //= 2
+        for r, b in enumerate(bands):
+            other = bands[1 - r].planes
+            b.planes[:, g - k:g, :] = other[:, g + B - k:g + B, :]
+            b.planes[:, g + B:g + B + k, :] = other[:, g:g + k, :]
+        for b in bands:
+            _abi.check(_abi.lib.cb2_band_pass_at(b.automaton, _planes(b.bufs[b.cur]), _planes(b.bufs[1 - b.cur]), x,
+                                                 b.rows_total, g, B, k, done, b.seed, b.row0 - g, rows,
+                                                 ctypes.byref(t), None))
+            b.cur ^= 1
+        left -= k
+        done += k
+    _, _, states = cb.automaton_info(name)
+    probs = [0.5, 0.25, 0.25] if states == 3 else [1.0 / states] * states
+    cells = O.init_cells(x, rows, seed, O.thresholds(probs))
+    want, want_ck = ref.ref_run_named(name, cells, steps, seed=9)
+    got = np.concatenate([O.unpack("bit_planes", b.band_planes_host().numpy().view(np.uint8).reshape(-1), x, B,
+                                   b.P, 32) for b in bands], axis=0)
+    assert (got == want).all()
+    sums = [sum(v) for v in zip(*[b.local_checksum() for b in bands])]
+    assert "-".join(str(v) for v in sums) == want_ck
+
+
+def test_band_grid_runs_dsl_automata_alone(ref):
+    # one rank: ghost rows from its own band, the generic BandGrid.run path
+    from cellato_b200.bands import BandGrid
+    x, rows, steps = 256, 80, 29
+    b = BandGrid("lightning-forest", x, rows)
+    b.fill_random(3, [0.3, 0.6, 0.1])
+    b.seed = 11
+    b.run(steps)
+    cells = O.init_cells(x, rows, 3, O.thresholds([0.3, 0.6, 0.1]))
+    want, want_ck = ref.ref_run_named("lightning-forest", cells, steps, seed=11)
+    got = O.unpack("bit_planes", b.band_planes_host().numpy().view(np.uint8).reshape(-1), x, rows, b.P, 32)
+    assert (got == want).all()
+    assert "-".join(str(v) for v in b.checksum()) == want_ck

@@ -72,3 +72,15 @@ def test_oracle_matches_reference_all_layouts(automaton):
                 assert (O.unpack(layout, packed, x, y, P, W) == cells).all()
                 rc, rck = O.ref_run(automaton, cells, steps, layout, W)
                 assert rck == ref_ck and (rc == ref_cells).all(), (layout, W)
+
+
+def test_thresholds_accept_decimal_probabilities_that_sum_to_one_within_rounding():
+    import cellato_b200 as cb
+    from fractions import Fraction
+    third = [1.0 / 3] * 3
+    assert (O.thresholds(third) == cb.thresholds(third)).all()
+    exact = O.thresholds([Fraction(1, 3)] * 3)
+    assert (exact == cb.thresholds([Fraction(1, 3)] * 3)).all()
+    assert list(exact) == [(1 << 53) // 3, (2 << 53) // 3]
+    with pytest.raises(ValueError):
+        O.thresholds([0.5, 0.4])
