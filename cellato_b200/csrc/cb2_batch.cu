@@ -23,8 +23,13 @@
 // tasks, so a broken schedule ends the kernel with an error status instead
 // of a hang.
 //
-// Order: chunk level by chunk level, and within a level the grids with the
-// most chunks first, so the longest dependency chains start earliest.
+// Order: by progress through the grid, (level + 1/2) / levels, so every
+// grid's chain of levels is spread over the whole run and the longest
+// chains do not run alone at the end; ties go to the grids with the most
+// chunks.  A grid's levels keep their order, so every task still waits only
+// for earlier tasks.  (Level-major order -- all grids' level c before any
+// level c+1 -- left a tail of a few long-running grids: 15.9 against 18.1
+// Tcell/s on 4096 mixed grids.)
 //
 // The launch (counter resets + kernel) is captured once in a CUDA graph and
 // replayed; the task count lives in device memory, so the same graph runs
@@ -225,7 +230,6 @@ int batch_engine::build(const std::vector<batch_item>& items, const batch_tiling
     };
     std::vector<plan_t> plans((size_t)n);
     std::vector<int> order((size_t)n);
-    int max_chunks = 0;
     for (int i = 0; i < n; ++i) {
         const batch_item& it = items[(size_t)i];
         const cb2_grid* g = it.grid;
@@ -238,7 +242,6 @@ int batch_engine::build(const std::vector<batch_item>& items, const batch_tiling
             p.ks.push_back(k);
             left -= k;
         }
-        max_chunks = std::max(max_chunks, (int)p.ks.size());
         const int wd = g->g.wd, h = g->g.h;
         const int rows = std::max(kmain, std::min(h, tiling.tile_rows));
         if (wd <= 16) {  // exact-wrap groups across the warp
@@ -269,10 +272,20 @@ int batch_engine::build(const std::vector<batch_item>& items, const batch_tiling
     std::vector<int> prev_base((size_t)n, -1);
     ntasks = 0;
     cells_per_run = 0;
-    for (int c = 0; c < max_chunks; ++c) {
-        for (int i : order) {
+    struct slot_t {
+        double progress;
+        int i, c;
+    };
+    std::vector<slot_t> slots;
+    for (int i : order)
+        for (int c = 0; c < (int)plans[(size_t)i].ks.size(); ++c)
+            slots.push_back(slot_t{(c + 0.5) / (double)plans[(size_t)i].ks.size(), i, c});
+    std::stable_sort(slots.begin(), slots.end(),
+                     [](const slot_t& x, const slot_t& y) { return x.progress < y.progress; });
+    for (const slot_t& sl : slots) {
+        const int i = sl.i, c = sl.c;
+        {
             const plan_t& p = plans[(size_t)i];
-            if (c >= (int)p.ks.size()) continue;
             const int per_chunk = p.nsx * p.nsy;
             if (ntasks + per_chunk > task_cap) return efail(CB2_ENOMEM, "batch task list is full");
             const int base = ntasks;
