@@ -1,14 +1,18 @@
 // cb2_batch.cu -- many independent grids in one persistent kernel.
 //
 // A batch advances each of its grids by that grid's own number of
-// generations.  The work is cut into tasks: one task = one warp running the
-// skewed single-warp wavefront (warp_run, cb2_pipe.cuh) over one strip of
-// one grid for one chunk of K generations.  Grids at most 16 words wide run
-// in group geometry: the warp holds several exact-wrap copies of the row,
-// each over its own rows, so narrow grids do not waste the warp on halo.
+// generations.  The work is cut into tasks: one task = one CTA running the
+// level pipeline (pipe_run_rows, cb2_pipe.cuh) over one strip of one grid
+// for one chunk of K generations, its K levels split over the CTA's four
+// warps, four rows per barrier.  Splitting the levels divides a task's
+// latency, and with it the length of a grid's chain of chunks, by four (a
+// task per warp: 15.9-18.0 Tcell/s; per CTA: 19.1 on the bench workload).
+// Grids at most 16 words wide run in group geometry: the lanes hold several
+// exact-wrap copies of the row, each over its own rows, so narrow grids do
+// not waste the warp on halo.
 //
 // The tasks sit in a device array in schedule order.  A persistent kernel
-// (one CTA per resident slot, every warp independent) takes tasks in that
+// (one CTA per resident slot, one task at a time) takes tasks in that
 // order from an atomic head index.  Chunk c of a grid reads buffer c&1 and
 // writes the other.  The tasks of every chunk of a grid tile it the same
 // way, and a task reads its own tile plus K rows and one word around it, so
@@ -52,9 +56,12 @@
 
 namespace cb2 {
 
-constexpr int kBatchWarps = 4;                                  // independent warps per CTA
-constexpr int kBatchPlanes = 3;                                  // the hand-written networks' largest P
-constexpr int kBatchSmemWords = kBatchPlanes * 32 * kRingDepth;  // one warp's input ring (V = 1)
+constexpr int kBatchWarps = 4;   // warps of a CTA: one task per CTA, its levels split over them
+constexpr int kBatchPlanes = 3;  // the hand-written networks' largest P
+constexpr int kBatchRows = 4;    // rows each warp passes on per barrier (2: 18.3, 4: 19.1 Tcell/s)
+// Shared memory of the largest task pipeline (K = 8 over the 4 warps, P = 3):
+// the input ring plus two four-row hand-off slots per warp boundary.
+constexpr int kBatchSmemWords = (kRingDepth + 2 * kBatchRows * (kBatchWarps - 1)) * kBatchPlanes * 32;
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
     unsigned v;
@@ -62,7 +69,7 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
     return v;
 }
 
-// Bounded wait until *p != 0; gives up early when another warp failed.
+// Bounded wait until *p != 0; gives up early when another CTA failed.
 __device__ __forceinline__ bool wait_flag(const unsigned* p, long long limit, const unsigned* error) {
     for (long long i = 0;; ++i) {
         if (ld_acquire(p) != 0) return true;
@@ -73,9 +80,21 @@ __device__ __forceinline__ bool wait_flag(const unsigned* p, long long limit, co
 
 __device__ __forceinline__ int wrap(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
 
+// One chunk of K generations of one task on the whole CTA: the level pipeline
+// of pipe_run_rows with the K levels split over the warps (K = 8: two levels
+// per warp, K = 4: one), which divides a task's latency -- and with it the
+// length of a grid's chain of chunks -- by the number of warps.  Chunks
+// shorter than the CTA (K = 2, 1) leave warps idle at the barriers.
 template <class R, int K>
 __device__ __forceinline__ void batch_run_task(const strip_task& t, const lane_geom<1>& geom, uint32_t* smem) {
-    warp_run<R, K, 1, kRingDepth>(t, geom, smem);
+    constexpr int L = K >= kBatchWarps ? K / kBatchWarps : 1;
+    constexpr int W = K / L;
+    static_assert(pipe_rows_smem_words<R, K, 1, L, kRingDepth, kBatchRows>() <= kBatchSmemWords,
+                  "task pipeline larger than the CTA's shared memory");
+    if ((int)(threadIdx.x >> 5) < W)
+        pipe_run_rows<R, K, 1, L, kRingDepth, kBatchRows>(t, geom, smem);
+    else
+        pipe_rows_idle<K, L, kBatchRows>(t);
 }
 
 template <class R, int KMAX>
@@ -92,31 +111,38 @@ __device__ __forceinline__ void batch_run_rule(const strip_task& t, int k, const
 
 template <int KMAX>
 __global__ void __launch_bounds__(kBatchWarps * 32) batch_kernel(batch_args a) {
-    __shared__ __align__(16) uint32_t smem_all[kBatchWarps * kBatchSmemWords];
+    __shared__ __align__(16) uint32_t smem[kBatchSmemWords];
+    __shared__ unsigned s_task;
+    __shared__ int s_ok;
     const int lane = threadIdx.x & 31;
-    uint32_t* smem = smem_all + (threadIdx.x >> 5) * kBatchSmemWords;
+    const int warp = threadIdx.x >> 5;
     const unsigned ntasks = *a.ntasks;
     for (;;) {
-        unsigned t = 0;
-        if (lane == 0) t = ld_acquire(a.error) ? UINT_MAX : atomicAdd(a.head, 1u);
-        t = __shfl_sync(kFullMask, t, 0);
-        if (t >= ntasks) break;
+        if (threadIdx.x == 0) s_task = ld_acquire(a.error) ? UINT_MAX : atomicAdd(a.head, 1u);
+        __syncthreads();
+        const unsigned t = s_task;
+        if (t >= ntasks) break;  // the same for the whole CTA
         const batch_task task = a.tasks[t];
         const batch_grid_desc gd = a.grids[task.grid];
-        // lanes 0..8 wait for the previous chunk's tasks on the 3x3 neighbouring tiles
+        // warp 0, lanes 0..8: the previous chunk's tasks on the 3x3 neighbouring tiles
         const unsigned* dep = a.task_done;
         if (task.dep_base >= 0) {
             const int j = lane < 9 ? lane : 4;  // lanes past the 3x3 tiles use the centre one
             const int dx = j % 3 - 1, dy = j / 3 - 1;
             dep += task.dep_base + wrap(task.ty + dy, task.nsy) * task.nsx + wrap(task.tx + dx, task.nsx);
         }
-        int ok = 1;
-        if (task.dep_base >= 0 && lane < 9) ok = wait_flag(dep, a.spin_limit, a.error);
-        if (!__all_sync(kFullMask, ok)) {
-            if (lane == 0) atomicCAS(a.error, 0u, t + 1);
-            break;
+        if (warp == 0) {
+            int ok = 1;
+            if (task.dep_base >= 0 && lane < 9) ok = wait_flag(dep, a.spin_limit, a.error);
+            ok = __all_sync(kFullMask, ok);
+            if (lane == 0) {
+                s_ok = ok;
+                if (!ok) atomicCAS(a.error, 0u, t + 1);
+            }
         }
-        if (task.dep_base >= 0 && lane >= 9) (void)ld_acquire(dep);  // acquire in every lane
+        __syncthreads();
+        if (!s_ok) break;
+        if (task.dep_base >= 0) (void)ld_acquire(dep);  // acquire in every thread
         strip_task st;
         st.in = gd.buf[task.chunk & 1];
         st.out = gd.buf[(task.chunk & 1) ^ 1];
@@ -144,9 +170,9 @@ __global__ void __launch_bounds__(kBatchWarps * 32) batch_kernel(batch_args a) {
         case 1: batch_run_rule<wire, KMAX>(st, task.k, geom, smem); break;
         default: batch_run_rule<excitable, KMAX>(st, task.k, geom, smem); break;
         }
-        __threadfence();  // this lane's stores are visible GPU-wide before the flag
-        __syncwarp();
-        if (lane == 0) atomicExch(a.task_done + t, 1u);
+        __threadfence();  // this thread's stores are visible GPU-wide before the flag
+        __syncthreads();  // every warp's stores are done; smem and s_task are free again
+        if (threadIdx.x == 0) atomicExch(a.task_done + t, 1u);
     }
 }
 

@@ -11,7 +11,7 @@
 
 namespace cb2 {
 
-// One warp's work: one strip (groups == 0) or `groups` exact-wrap copies of a
+// One CTA's work: one strip (groups == 0) or `groups` exact-wrap copies of a
 // narrow grid's row (groups > 0), for one chunk of k generations.  The tasks
 // of a chunk tile the grid as nsy rows of nsx tasks; (tx, ty) is this one.
 struct batch_task {
@@ -93,8 +93,7 @@ struct batch_engine {
     // stream passed it, error_seen() reports it without synchronising.
     int read_error_async(cudaStream_t s);
     int error_seen();
-
-private:
+    // Captures the launch graph now (launch does it on first use otherwise).
     int capture();
 };
 

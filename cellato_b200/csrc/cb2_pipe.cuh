@@ -178,7 +178,7 @@ __device__ __forceinline__ void pipe_run(const strip_task& t, uint32_t* smem) {
 // Shared memory of pipe_run_rows in 32-bit words: the input ring plus two
 // RPS-row hand-off slots per warp boundary.
 template <class R, int K, int V, int L, int DEPTH, int RPS>
-constexpr int pipe_rows_smem_words() {
+__host__ __device__ constexpr int pipe_rows_smem_words() {
     return (DEPTH + 2 * RPS * (K / L - 1)) * R::P * 32 * V;
 }
 
@@ -188,7 +188,7 @@ constexpr int pipe_rows_smem_words() {
 // slot j & 1, so no step parity is needed.  cp.async groups hold RPS rows;
 // the ring of DEPTH rows keeps DEPTH / RPS - 1 groups in flight.
 template <class R, int K, int V, int L, int DEPTH, int RPS>
-__device__ __forceinline__ void pipe_run_rows(const strip_task& t, uint32_t* smem) {
+__device__ __forceinline__ void pipe_run_rows(const strip_task& t, const lane_geom<V>& geom, uint32_t* smem) {
     static_assert(K % L == 0, "levels per warp must divide K");
     static_assert(K <= 32, "the one-word halo of a strip covers at most 32 generations");
     static_assert(RPS >= 2 && RPS % 2 == 0, "an even number of rows per step");
@@ -199,7 +199,6 @@ __device__ __forceinline__ void pipe_run_rows(const strip_task& t, uint32_t* sme
     constexpr int G = DEPTH / RPS;    // groups of RPS rows in the ring
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const lane_geom<V> geom = strip_geom<V>(t, lane);
 
     strip_state<R, L, V> s;
 #pragma unroll
@@ -238,7 +237,7 @@ __device__ __forceinline__ void pipe_run_rows(const strip_task& t, uint32_t* sme
         cp_async_commit();
     };
     if (warp == 0) {
-        lr = (t.y0 - K) % t.h;
+        lr = (t.y0 + geom.yoff - K) % t.h;  // a lane of a narrow grid's row group starts at its own rows
         if (lr < 0) lr += t.h;
 #pragma unroll
         for (int g = 0; g < G - 1; ++g) issue(g);
@@ -297,6 +296,22 @@ __device__ __forceinline__ void pipe_run_rows(const strip_task& t, uint32_t* sme
         __syncthreads();
     }
     if (warp == 0) cp_async_wait<0>();
+}
+
+// pipe_run_rows over the strip geometry of the task.
+template <class R, int K, int V, int L, int DEPTH, int RPS>
+__device__ __forceinline__ void pipe_run_rows(const strip_task& t, uint32_t* smem) {
+    pipe_run_rows<R, K, V, L, DEPTH, RPS>(t, strip_geom<V>(t, threadIdx.x & 31), smem);
+}
+
+// The barriers of pipe_run_rows<R, K, V, L, DEPTH, RPS> for a warp of the
+// CTA beyond its K / L pipeline warps (a CTA sized for longer chains running
+// a short one): it takes part in every __syncthreads and touches nothing.
+template <int K, int L, int RPS>
+__device__ __forceinline__ void pipe_rows_idle(const strip_task& t) {
+    const int steps = (t.ny + 2 * K + RPS - 1) / RPS + K / L - 1;
+    __syncthreads();
+    for (int st = 0; st < steps; ++st) __syncthreads();
 }
 
 // Shared memory of one warp-strip (skewed single-warp kernel) in 32-bit words.
