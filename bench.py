@@ -186,9 +186,15 @@ def traffic_for(kernel_key: str):
 BATCH_PROBS = {0: [0.65, 0.35], 1: [0.60, 0.05, 0.05, 0.30], 2: [0.125] * 8}
 
 
-def batch_workload(n: int, seed: int = 2024):
-    """4096 independent grids: sides log-uniform in [64, 4096] (widths rounded to
-    multiples of 32), automaton uniform over the three, steps log-uniform in
+# The lowered DSL automata of the batched DSL line: every bundled automaton
+# without a hand-written network and the two stochastic examples.
+BATCH_DSL = ["brian", "critters", "cyclic", "forest-fire", "fluid", "maze", "traffic", "lightning-forest",
+             "noisy-life"]
+
+
+def batch_workload(n: int, seed: int = 2024, automata=(0, 1, 2)):
+    """n independent grids: sides log-uniform in [64, 4096] (widths rounded to
+    multiples of 32), automaton uniform over `automata`, steps log-uniform in
     [10, 1000]."""
     import numpy as np
 
@@ -198,18 +204,26 @@ def batch_workload(n: int, seed: int = 2024):
     for i in range(n):
         x = int(min(4096, max(64, 32 * round(math.exp(rng.uniform(lo, hi)) / 32))))
         y = int(min(4096, max(64, round(math.exp(rng.uniform(lo, hi))))))
-        a = int(rng.integers(0, 3))
+        a = automata[int(rng.integers(0, len(automata)))]
         steps = int(round(math.exp(rng.uniform(math.log(10), math.log(1000)))))
         specs.append((a, x, y, steps))
     return specs
 
 
-def bench_batch(cb, torch, stream, n: int, runs: int) -> dict:
-    specs = batch_workload(n)
+def batch_probs(cb, a):
+    if a in BATCH_PROBS:
+        return BATCH_PROBS[a]
+    states = cb.automaton_info(a)[2]
+    return [0.5, 0.25, 0.25] if states == 3 else [1.0 / states] * states  # exact binary fractions
+
+
+def bench_batch(cb, torch, stream, n: int, runs: int, automata=(0, 1, 2)) -> dict:
+    specs = batch_workload(n, automata=automata)
     grids = []
     for i, (a, x, y, _) in enumerate(specs):
         g = cb.DeviceGrid(a, x, y)
-        g.fill_random(1000 + i, BATCH_PROBS[a], stream=stream)
+        g.fill_random(1000 + i, batch_probs(cb, a), stream=stream)
+        g.set_seed(5000 + i)
         grids.append(g)
     steps = [s for (_, _, _, s) in specs]
     batch = cb.Batch(grids, steps)
@@ -236,8 +250,9 @@ def bench_batch(cb, torch, stream, n: int, runs: int) -> dict:
     for g in grids:
         g.close()
     cells = info["cell_updates"]
+    names = ", ".join(cb.automaton_info(a)[0] if isinstance(a, int) else a for a in automata)
     return {"workload": f"{n} grids, sides log-uniform [64,4096] (widths multiple of 32), automaton uniform "
-                        "{game-of-life, wire, excitable}, steps log-uniform [10,1000], seeded inits",
+                        f"{{{names}}}, steps log-uniform [10,1000], seeded inits",
             "value": cells / (ms * 1e-3) / 1e9, "unit": METRIC, "ms_per_run": ms, "runs": runs,
             "cell_updates_per_run": cells, "tasks": info["tasks"], "persistent_ctas": info["persistent_ctas"],
             "per_grid_value": cells / (per_ms * 1e-3) / 1e9, "per_grid_ms_per_run": per_ms,
@@ -338,6 +353,8 @@ def main() -> None:
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=300)
     ap.add_argument("--batch-grids", type=int, default=4096)
+    ap.add_argument("--batch-dsl-grids", type=int, default=1024,
+                    help="grids of the batched line over the lowered DSL automata (0 = skip)")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
@@ -492,6 +509,9 @@ def main() -> None:
     batched = None
     if not args.no_batch:
         batched = bench_batch(cb, torch, stream, args.batch_grids, max(3, args.steps))
+    batched_dsl = None
+    if not args.no_batch and args.batch_dsl_grids > 0 and all(n in cb.AUTOMATA for n in BATCH_DSL):
+        batched_dsl = bench_batch(cb, torch, stream, args.batch_dsl_grids, 3, automata=BATCH_DSL)
     served = None
     if not args.no_serve:
         served = bench_serve(cb, args.serve_requests, [100.0, 1000.0, 5000.0, 20000.0])
@@ -525,6 +545,7 @@ def main() -> None:
         "clocks": clocks,
         "cpu_baseline": cpu,
         "batched": batched,
+        "batched_dsl": batched_dsl,
         "served": served,
     }
     print(json.dumps(out), flush=True)

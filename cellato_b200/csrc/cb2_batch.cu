@@ -38,6 +38,14 @@
 // The launch (counter resets + kernel) is captured once in a CUDA graph and
 // replayed; the task count lives in device memory, so the same graph runs
 // any task list up to the engine's capacity (the serving loop relies on it).
+//
+// Two kernels share this schedule (cb2_batch_kernel.cuh): one over the
+// hand-written networks alone, here, and one over every registered
+// automaton, cb2_generic_batch.cu, which a batch holding a lowered DSL
+// automaton runs.  There a task also takes its chunk's first generation
+// (from the grid's run start and its chunk split) and the grid's seed, which
+// stochastic and time-dependent rules read; the run start advances on the
+// device after each run, so replays continue the grids' time.
 #include "cellato_b200.h"
 
 #include <cuda_runtime.h>
@@ -50,145 +58,50 @@
 #include <vector>
 
 #include "cb2_batch.h"
+#include "cb2_batch_kernel.cuh"
 #include "cb2_internal.h"
-#include "cb2_pipe.cuh"
 #include "cb2_rules.cuh"
 
 namespace cb2 {
 
-constexpr int kBatchWarps = 4;   // warps of a CTA: one task per CTA, its levels split over them
-constexpr int kBatchPlanes = 3;  // the hand-written networks' largest P
-constexpr int kBatchRows = 4;    // rows each warp passes on per barrier (2: 18.3, 4: 19.1 Tcell/s)
-// Shared memory of the largest task pipeline (K = 8 over the 4 warps, P = 3):
-// the input ring plus two four-row hand-off slots per warp boundary.
-constexpr int kBatchSmemWords = (kRingDepth + 2 * kBatchRows * (kBatchWarps - 1)) * kBatchPlanes * 32;
+constexpr int kBuiltinPlanes = 3;  // the hand-written networks' largest P
+constexpr int kBuiltinRows = 4;    // rows each warp passes on per barrier (2: 18.3, 4: 19.1 Tcell/s)
 
-__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-// Bounded wait until *p != 0; gives up early when another CTA failed.
-__device__ __forceinline__ bool wait_flag(const unsigned* p, long long limit, const unsigned* error) {
-    for (long long i = 0;; ++i) {
-        if (ld_acquire(p) != 0) return true;
-        if (i >= limit || ld_acquire(error) != 0) return false;
-        __nanosleep(i < 32 ? 64 : 512);
-    }
-}
-
-__device__ __forceinline__ int wrap(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
-
-// One chunk of K generations of one task on the whole CTA: the level pipeline
-// of pipe_run_rows with the K levels split over the warps (K = 8: two levels
-// per warp, K = 4: one), which divides a task's latency -- and with it the
-// length of a grid's chain of chunks -- by the number of warps.  Chunks
-// shorter than the CTA (K = 2, 1) leave warps idle at the barriers.
-template <class R, int K>
-__device__ __forceinline__ void batch_run_task(const strip_task& t, const lane_geom<1>& geom, uint32_t* smem) {
-    constexpr int L = K >= kBatchWarps ? K / kBatchWarps : 1;
-    constexpr int W = K / L;
-    static_assert(pipe_rows_smem_words<R, K, 1, L, kRingDepth, kBatchRows>() <= kBatchSmemWords,
-                  "task pipeline larger than the CTA's shared memory");
-    if ((int)(threadIdx.x >> 5) < W)
-        pipe_run_rows<R, K, 1, L, kRingDepth, kBatchRows>(t, geom, smem);
-    else
-        pipe_rows_idle<K, L, kBatchRows>(t);
-}
-
-template <class R, int KMAX>
-__device__ __forceinline__ void batch_run_rule(const strip_task& t, int k, const lane_geom<1>& geom, uint32_t* smem) {
-    switch (k) {
-    case 1: batch_run_task<R, 1>(t, geom, smem); break;
-    case 2: batch_run_task<R, 2>(t, geom, smem); break;
-    case 4: batch_run_task<R, 4>(t, geom, smem); break;
-    default:
-        if constexpr (KMAX >= 8) batch_run_task<R, 8>(t, geom, smem);
-        break;
-    }
-}
-
+// The hand-written networks: the kernel of kind kBatchBuiltin.  KMAX = 4
+// drops the eight-generation pipelines (a batch whose chunks are at most 4).
 template <int KMAX>
-__global__ void __launch_bounds__(kBatchWarps * 32) batch_kernel(batch_args a) {
-    __shared__ __align__(16) uint32_t smem[kBatchSmemWords];
-    __shared__ unsigned s_task;
-    __shared__ int s_ok;
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    const unsigned ntasks = *a.ntasks;
-    for (;;) {
-        if (threadIdx.x == 0) s_task = ld_acquire(a.error) ? UINT_MAX : atomicAdd(a.head, 1u);
-        __syncthreads();
-        const unsigned t = s_task;
-        if (t >= ntasks) break;  // the same for the whole CTA
-        const batch_task task = a.tasks[t];
-        const batch_grid_desc gd = a.grids[task.grid];
-        // warp 0, lanes 0..8: the previous chunk's tasks on the 3x3 neighbouring tiles
-        const unsigned* dep = a.task_done;
-        if (task.dep_base >= 0) {
-            const int j = lane < 9 ? lane : 4;  // lanes past the 3x3 tiles use the centre one
-            const int dx = j % 3 - 1, dy = j / 3 - 1;
-            dep += task.dep_base + wrap(task.ty + dy, task.nsy) * task.nsx + wrap(task.tx + dx, task.nsx);
+struct builtin_rules {
+    static constexpr int kSmemWords = batch_smem_words(kBuiltinPlanes, kBuiltinRows);
+    static constexpr bool kTimed = false;  // the networks read neither time, seed nor global rows
+    __device__ __forceinline__ static void run(int automaton, int k, const strip_task& t, const lane_geom<1>& geom,
+                                               uint32_t* smem) {
+        switch (automaton) {
+        case 0: batch_run_rule<game_of_life, KMAX, kBuiltinRows, kSmemWords>(t, k, geom, smem); break;
+        case 1: batch_run_rule<wire, KMAX, kBuiltinRows, kSmemWords>(t, k, geom, smem); break;
+        default: batch_run_rule<excitable, KMAX, kBuiltinRows, kSmemWords>(t, k, geom, smem); break;
         }
-        if (warp == 0) {
-            int ok = 1;
-            if (task.dep_base >= 0 && lane < 9) ok = wait_flag(dep, a.spin_limit, a.error);
-            ok = __all_sync(kFullMask, ok);
-            if (lane == 0) {
-                s_ok = ok;
-                if (!ok) atomicCAS(a.error, 0u, t + 1);
-            }
-        }
-        __syncthreads();
-        if (!s_ok) break;
-        if (task.dep_base >= 0) (void)ld_acquire(dep);  // acquire in every thread
-        strip_task st;
-        st.in = gd.buf[task.chunk & 1];
-        st.out = gd.buf[(task.chunk & 1) ^ 1];
-        st.plane_words = gd.plane_words;
-        st.t0 = 0;  // the hand-written networks read neither time, seed nor global rows
-        st.seed = 0;
-        st.y_global0 = 0;
-        st.global_h = gd.h;
-        st.wd = gd.wd;
-        st.h = gd.h;
-        lane_geom<1> geom;
-        st.y0 = task.y0;
-        st.ny = task.rows;
-        if (task.groups) {
-            st.x0 = 0;
-            st.nx = gd.wd;
-            geom = group_geom(st, task.groups, lane);
-        } else {
-            st.x0 = task.tx * 30;
-            st.nx = min(30, gd.wd - st.x0);
-            geom = strip_geom<1>(st, lane);
-        }
-        switch (gd.automaton) {
-        case 0: batch_run_rule<game_of_life, KMAX>(st, task.k, geom, smem); break;
-        case 1: batch_run_rule<wire, KMAX>(st, task.k, geom, smem); break;
-        default: batch_run_rule<excitable, KMAX>(st, task.k, geom, smem); break;
-        }
-        __threadfence();  // this thread's stores are visible GPU-wide before the flag
-        __syncthreads();  // every warp's stores are done; smem and s_task are free again
-        if (threadIdx.x == 0) atomicExch(a.task_done + t, 1u);
     }
-}
+};
 
 // After a run, a grid that took an odd number of chunks holds its result in
-// buffer 1: swap so that buffer 0 is again the current generation.
-__global__ void batch_flip_kernel(batch_grid_desc* grids, const unsigned char* odd, int n) {
+// buffer 1: swap so that buffer 0 is again the current generation.  Every
+// grid's generation advances by its steps, so a replay of the same schedule
+// continues the grids' time.
+__global__ void batch_flip_kernel(batch_grid_desc* grids, const unsigned char* odd, const unsigned* n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n && odd[i]) {
-        uint32_t* t = grids[i].buf[0];
-        grids[i].buf[0] = grids[i].buf[1];
-        grids[i].buf[1] = t;
+    if (i < (int)*n) {
+        if (odd[i]) {
+            uint32_t* t = grids[i].buf[0];
+            grids[i].buf[0] = grids[i].buf[1];
+            grids[i].buf[1] = t;
+        }
+        grids[i].t0 += grids[i].steps;
     }
 }
 
-static const void* batch_kernel_for(int kmax) {
-    return kmax >= 8 ? (const void*)batch_kernel<8> : (const void*)batch_kernel<4>;
+static const void* batch_kernel_for(int kind, int kmax) {
+    if (kind == kBatchAll) return generic_batch_kernel();
+    return kmax >= 8 ? (const void*)batch_kernel<builtin_rules<8>> : (const void*)batch_kernel<builtin_rules<4>>;
 }
 
 // ---- engine -------------------------------------------------------------------------------------
@@ -222,17 +135,23 @@ int batch_engine::init(int task_capacity, int grid_capacity, int kmax_, long lon
     if (e == cudaSuccess) e = cudaMemset(d_odd, 0, (size_t)grid_cap);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return ecuda(e, "batch engine allocation");
-    const void* fn = batch_kernel_for(kmax);
-    int per_sm = 0, sms = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBatchWarps * 32, 0);
+    int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    blocks = std::max(1, per_sm) * std::max(1, sms);
+    for (int k = 0; k < 2; ++k) {
+        const void* fn = batch_kernel_for(k, kmax);
+        int per_sm = 0;
+        if (fn) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBatchWarps * 32, 0);
+        kind_blocks[k] = std::max(1, per_sm) * std::max(1, sms);
+    }
+    blocks = kind_blocks[kBatchBuiltin];
     return CB2_OK;
 }
 
 void batch_engine::release() {
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
+    for (int k = 0; k < 2; ++k) {
+        if (exec[k]) cudaGraphExecDestroy(exec[k]);
+        if (graph[k]) cudaGraphDestroy(graph[k]);
+    }
     if (cap_stream) cudaStreamDestroy(cap_stream);
     cudaFree(d_tasks);
     cudaFree(d_grids);
@@ -256,12 +175,14 @@ int batch_engine::build(const std::vector<batch_item>& items, const batch_tiling
     };
     std::vector<plan_t> plans((size_t)n);
     std::vector<int> order((size_t)n);
+    kind = kBatchBuiltin;
     for (int i = 0; i < n; ++i) {
         const batch_item& it = items[(size_t)i];
         const cb2_grid* g = it.grid;
         plan_t& p = plans[(size_t)i];
         int64_t left = it.steps;
         const int kmain = std::min(kmax, tiling.temporal_steps > 0 ? tiling.temporal_steps : kmax);
+        if (it.steps / kmain > INT_MAX) return efail(CB2_EINVAL, "too many generations for one batch run");
         while (left > 0) {
             int k = kmain;
             while (k > left) k /= 2;
@@ -289,7 +210,13 @@ int batch_engine::build(const std::vector<batch_item>& items, const batch_tiling
         d.wd = wd;
         d.h = h;
         d.automaton = g->g.automaton;
-        d.pad = 0;
+        d.t0 = it.t0;
+        d.seed = it.seed;
+        d.steps = it.steps;
+        d.kmain = kmain;
+        d.nfull = (int32_t)(it.steps / kmain);
+        d.rem = (int32_t)(it.steps % kmain);
+        if (d.automaton >= kNumBuiltin) kind = kBatchAll;
         h_odd[i] = (unsigned char)(p.ks.size() & 1);
         order[(size_t)i] = i;
     }
@@ -345,22 +272,30 @@ int batch_engine::build(const std::vector<batch_item>& items, const batch_tiling
         }
     }
     ngrids = n;
+    if (kind == kBatchAll && !generic_batch_kernel())
+        return efail(CB2_EINVAL, "the library was built without the lowered DSL automata");
+    blocks = kind_blocks[kind];
     return CB2_OK;
 }
 
 int batch_engine::upload(cudaStream_t s) {
     h_misc[0] = (unsigned)ntasks;
+    h_misc[2] = (unsigned)ngrids;
     cudaError_t e = cudaMemcpyAsync(d_tasks, h_tasks, sizeof(batch_task) * (size_t)ntasks, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(d_grids, h_grids, sizeof(batch_grid_desc) * (size_t)ngrids, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_odd, h_odd, (size_t)ngrids, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_counters + 3, h_misc, sizeof(unsigned), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_counters + 2, h_misc + 2, sizeof(unsigned), cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return ecuda(e, "batch task upload");
     return CB2_OK;
 }
 
-int batch_engine::capture() {
-    if (exec) return CB2_OK;
+int batch_engine::capture(int k) {
+    if (k != kBatchBuiltin && k != kBatchAll) return efail(CB2_EINVAL, "unknown batch kernel kind");
+    if (exec[k]) return CB2_OK;
+    const void* fn = batch_kernel_for(k, kmax);
+    if (!fn) return efail(CB2_EINVAL, "the library was built without the lowered DSL automata");
     batch_args a;
     a.tasks = d_tasks;
     a.ntasks = d_counters + 3;
@@ -371,23 +306,23 @@ int batch_engine::capture() {
     a.spin_limit = spin_limit;
     cudaError_t e = cudaStreamBeginCapture(cap_stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return ecuda(e, "batch graph capture");
-    cudaMemsetAsync(d_counters, 0, sizeof(unsigned) * 3, cap_stream);
+    cudaMemsetAsync(d_counters, 0, sizeof(unsigned) * 2, cap_stream);  // head, error
     cudaMemsetAsync(d_task_done, 0, sizeof(unsigned) * (size_t)task_cap, cap_stream);
     void* args[] = {&a};
-    cudaLaunchKernel(batch_kernel_for(kmax), dim3((unsigned)blocks), dim3(kBatchWarps * 32), args, 0, cap_stream);
+    cudaLaunchKernel(fn, dim3((unsigned)kind_blocks[k]), dim3(kBatchWarps * 32), args, 0, cap_stream);
     const int nflip = grid_cap;
-    batch_flip_kernel<<<(nflip + 255) / 256, 256, 0, cap_stream>>>(d_grids, d_odd, nflip);
-    e = cudaStreamEndCapture(cap_stream, &graph);
+    batch_flip_kernel<<<(nflip + 255) / 256, 256, 0, cap_stream>>>(d_grids, d_odd, d_counters + 2);
+    e = cudaStreamEndCapture(cap_stream, &graph[k]);
     if (e != cudaSuccess) return ecuda(e, "batch graph capture");
-    e = cudaGraphInstantiate(&exec, graph, 0);
+    e = cudaGraphInstantiate(&exec[k], graph[k], 0);
     if (e != cudaSuccess) return ecuda(e, "batch graph instantiate");
     return CB2_OK;
 }
 
 int batch_engine::launch(cudaStream_t s) {
-    int rc = capture();
+    int rc = capture(kind);
     if (rc) return rc;
-    cudaError_t e = cudaGraphLaunch(exec, s);
+    cudaError_t e = cudaGraphLaunch(exec[kind], s);
     if (e != cudaSuccess) return ecuda(e, "batch graph launch");
     return CB2_OK;
 }
@@ -445,12 +380,7 @@ int cb2_batch_create(cb2_grid* const* grids, const int64_t* steps, int n, const 
             delete b;
             return efail(CB2_EINVAL, "null grid or negative steps in batch");
         }
-        if (grids[i]->g.automaton >= kNumBuiltin) {
-            delete b;
-            return efail(CB2_EINVAL, std::string("the batch kernel runs game-of-life, wire and excitable; '") +
-                                         name_of(grids[i]->g.automaton) + "' advances with cb2_grid_run");
-        }
-        b->items.push_back(batch_item{grids[i], steps[i], grids[i]->cur});
+        b->items.push_back(batch_item{grids[i], steps[i], grids[i]->cur, grids[i]->time_step, grids[i]->seed});
         const cb2_grid* g = grids[i];
         const int64_t chunks = steps[i] / std::max(1, b->tiling.temporal_steps) + 4;
         const int64_t rows = std::max<int64_t>(1, std::min<int64_t>(g->g.h, b->tiling.tile_rows));
@@ -490,9 +420,12 @@ int cb2_batch_run(cb2_batch* b, void* stream) {
     if (!b) return efail(CB2_EINVAL, "null batch");
     cudaStream_t s = (cudaStream_t)stream;
     for (batch_item& it : b->items)
-        if (it.grid->cur != it.cur) {  // the grid was advanced or re-uploaded outside the batch
+        if (it.grid->cur != it.cur || it.grid->time_step != it.t0 || it.grid->seed != it.seed) {
+            // the grid was advanced, re-uploaded, re-timed or re-seeded outside the batch
             b->built = false;
             it.cur = it.grid->cur;
+            it.t0 = it.grid->time_step;
+            it.seed = it.grid->seed;
         }
     if (!b->built) {
         // the pinned task list may still feed an earlier upload on this stream
@@ -516,6 +449,7 @@ int cb2_batch_run(cb2_batch* b, void* stream) {
             it.cur = it.grid->cur;
         }
         it.grid->time_step += it.steps;
+        it.t0 = it.grid->time_step;  // as batch_flip_kernel advances the device copy
     }
     return CB2_OK;
 }

@@ -32,8 +32,13 @@ static_assert(sizeof(batch_task) == 32, "batch_task is one 32-byte sector");
 struct batch_grid_desc {
     uint32_t* buf[2];  // buf[0] holds the current generation when a run starts
     int64_t plane_words;
+    int64_t t0;     // generation of the grid when the run starts (advanced on the device after each run)
+    uint64_t seed;  // random seed of stochastic rules
+    int64_t steps;  // generations of a run
     int32_t wd, h;
-    int32_t automaton, pad;
+    int32_t automaton;
+    int32_t kmain;  // K of the full chunks; nfull of them, then the remainder rem < kmain
+    int32_t nfull, rem;
 };
 
 struct batch_args {
@@ -49,7 +54,9 @@ struct batch_args {
 struct batch_item {
     cb2_grid* grid;
     int64_t steps;
-    int cur;  // the grid's current buffer when the schedule was built
+    int cur;        // the grid's current buffer when the schedule was built
+    int64_t t0;     // the grid's generation when the schedule was built
+    uint64_t seed;  // and its random seed
 };
 
 struct batch_tiling {
@@ -57,15 +64,26 @@ struct batch_tiling {
     int tile_rows = 256;     // output rows per strip task
 };
 
-// Device task list, counters and the captured launch graph.
+// The two kernels of a batch: the hand-written networks alone, or every
+// registered automaton (the lowered DSL rules need more registers and shared
+// memory, so they get a kernel of their own).
+enum batch_kind { kBatchBuiltin = 0, kBatchAll = 1 };
+
+// The kernel of kind kBatchAll (cb2_generic_batch.cu); null when the library
+// has no lowered DSL automata.
+const void* generic_batch_kernel();
+
+// Device task list, counters and the captured launch graphs.
 struct batch_engine {
     int device = 0;
     int kmax = 8;
     long long spin_limit = 0;
     int task_cap = 0, grid_cap = 0;
     int ntasks = 0, ngrids = 0;
+    int kind = kBatchBuiltin;  // the kernel the built schedule needs
     double cells_per_run = 0;
-    int blocks = 0;  // persistent CTAs
+    int blocks = 0;           // persistent CTAs of the kernel of `kind`
+    int kind_blocks[2] = {0, 0};
     batch_task* d_tasks = nullptr;
     batch_grid_desc* d_grids = nullptr;
     unsigned char* d_odd = nullptr;
@@ -76,8 +94,8 @@ struct batch_engine {
     unsigned char* h_odd = nullptr;
     unsigned* h_misc = nullptr;
     cudaStream_t cap_stream = nullptr;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph[2] = {nullptr, nullptr};  // per kind
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
 
     int init(int task_capacity, int grid_capacity, int kmax, long long spin_limit);
     void release();
@@ -85,7 +103,8 @@ struct batch_engine {
     int build(const std::vector<batch_item>& items, const batch_tiling& tiling);
     // Copies the schedule to the device (asynchronous on s).
     int upload(cudaStream_t s);
-    // Replays the captured graph (captures it on first use) on s.
+    // Replays the captured graph of the schedule's kind (captures it on first
+    // use) on s.
     int launch(cudaStream_t s);
     // Waits for s and reports a timed-out wait as CB2_ETIMEOUT.
     int check(cudaStream_t s);
@@ -93,8 +112,9 @@ struct batch_engine {
     // stream passed it, error_seen() reports it without synchronising.
     int read_error_async(cudaStream_t s);
     int error_seen();
-    // Captures the launch graph now (launch does it on first use otherwise).
-    int capture();
+    // Captures the launch graph of a kind now (launch does it on first use
+    // otherwise).  kBatchAll fails when there are no lowered DSL automata.
+    int capture(int kind = kBatchBuiltin);
 };
 
 } // namespace cb2

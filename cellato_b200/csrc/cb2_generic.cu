@@ -24,25 +24,9 @@
 #include <vector>
 
 #include "cb2_ast.cuh"
+#include "cb2_dsl_configs.h"
 #include "cb2_internal.h"
 #include "cb2_launch.cuh"
-
-#include "brian/config.hpp"
-#include "critters/config.hpp"
-#include "cyclic/config.hpp"
-#include "excitable/config.hpp"
-#include "fire/config.hpp"
-#include "fluid/config.hpp"
-#include "game_of_life/config.hpp"
-#include "maze/config.hpp"
-#include "traffic/config.hpp"
-#include "wire/config.hpp"
-
-#include "cellato_b200/dsl_examples.hpp"
-
-#ifdef CB2_USER_AUTOMATA
-#include CB2_USER_AUTOMATA
-#endif
 
 namespace cb2 {
 namespace {
@@ -93,18 +77,9 @@ void add(dsl_table& t, const char* name) {
 const dsl_table& table() {
     static const dsl_table t = [] {
         dsl_table d;
-        add<brian::config>(d, brian::config::name);
-        add<critters::config>(d, critters::config::name);
-        add<cyclic::config>(d, cyclic::config::name);
-        add<fire::config>(d, fire::config::name);
-        add<fluid::config>(d, fluid::config::name);
-        add<maze::config>(d, maze::config::name);
-        add<traffic::config>(d, traffic::config::name);
-        add<cellato_b200::examples::forest_fire_config>(d, cellato_b200::examples::forest_fire_config::name);
-        add<cellato_b200::examples::noisy_life_config>(d, cellato_b200::examples::noisy_life_config::name);
-        add<::game_of_life::config>(d, "game-of-life:dsl");
-        add<::wire::config>(d, "wire:dsl");
-        add<::excitable::config>(d, "excitable:dsl");
+#define CB2_ADD_CONFIG(C, NAME) add<C>(d, NAME);
+        CB2_DSL_CONFIGS(CB2_ADD_CONFIG)
+#undef CB2_ADD_CONFIG
 #ifdef CB2_USER_CONFIGS
 #define CB2_ADD_USER_CONFIG(C) add<C>(d, C::name);
         CB2_USER_CONFIGS(CB2_ADD_USER_CONFIG)

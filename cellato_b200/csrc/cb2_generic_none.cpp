@@ -3,6 +3,7 @@
 // and the hand-written networks (ids 0-2) are all the library runs.
 #include <vector>
 
+#include "cb2_batch.h"
 #include "cb2_internal.h"
 
 namespace cb2 {
@@ -15,5 +16,7 @@ const std::vector<strip_variant>& generic_variants(int) {
     static const std::vector<strip_variant> none;
     return none;
 }
+
+const void* generic_batch_kernel() { return nullptr; }
 
 } // namespace cb2

@@ -273,8 +273,9 @@ __device__ __forceinline__ void pipe_run_rows(const strip_task& t, const lane_ge
             if constexpr (R::kWindow) {
                 // warp w's chain receives sweep row RPS*st + j - w*(RPS + L) (warp w-1's
                 // output of the previous step, L rows behind its input)
-                row_ctx rc{t.t0 + (int64_t)warp * L, RPS * st + j - warp * (RPS + L), t.y0 - K, t.h, t.seed,
-                           t.y_global0, t.global_h};
+                // (a lane of a narrow grid's row group sweeps from its own first row)
+                row_ctx rc{t.t0 + (int64_t)warp * L, RPS * st + j - warp * (RPS + L), t.y0 + geom.yoff - K, t.h,
+                           t.seed, t.y_global0, t.global_h};
                 strip_push<R, L, V, 0>(s, rows[j], geom.src_l, geom.src_r, &geom, &rc);
                 rc.sweep += 1;
                 strip_push<R, L, V, 1>(s, rows[j + 1], geom.src_l, geom.src_r, &geom, &rc);

@@ -10,7 +10,9 @@
 //           the device.
 //   round   every active request advances up to chunk_steps generations in
 //           one replay of a batch engine's graph (cb2_batch.cu): one
-//           persistent kernel over all their tasks.  Requests of at least
+//           persistent kernel over all their tasks (the kernel over every
+//           automaton when the round holds a lowered DSL rule, with each
+//           request's generation and seed).  Requests of at least
 //           direct_cells cells instead advance through the single-grid strip
 //           kernels (cb2_grid_run's plan: up to 32 generations per HBM round
 //           trip, one CTA of several warps per strip) on side streams (each
@@ -144,7 +146,6 @@ struct server_impl {
     int init_grid(request_state* r);
     int retire(request_state* r);
     bool is_direct(const request_state* r) const {
-        if (r->req.automaton >= kNumBuiltin) return true;  // lowered DSL rules run in the strip kernels only
         return opts.direct_cells > 0 && (double)r->req.x_size * (double)r->req.y_size >= (double)opts.direct_cells;
     }
     cudaError_t enqueue_result(request_state* r, cudaStream_t s);
@@ -367,7 +368,8 @@ void server_impl::launch_round() {
         if (is_direct(r)) {
             direct_items.push_back({r, steps});
         } else {
-            items.push_back(batch_item{&r->grid, steps, r->grid.cur});
+            // generations already planned and the request's seed, for time- and seed-dependent rules
+            items.push_back(batch_item{&r->grid, steps, r->grid.cur, r->planned, r->req.seed});
             in_round.push_back(r);
         }
     }
@@ -688,7 +690,8 @@ int cb2_server_create(const cb2_server_opts* opts, cb2_server** out) {
     // ~0.2 s to every latency of a burst of arrivals).
     for (int i = 0; i < 2 && !m.opts.per_request; ++i) {
         int rc = m.engs[i].init(m.opts.task_capacity, m.opts.max_active, m.tiling.temporal_steps, m.opts.spin_limit);
-        if (!rc) rc = m.engs[i].capture();
+        if (!rc) rc = m.engs[i].capture(kBatchBuiltin);
+        if (!rc && generic_batch_kernel()) rc = m.engs[i].capture(kBatchAll);  // rounds holding lowered DSL rules
         if (rc) {
             for (int j = 0; j <= i; ++j) m.engs[j].release();
             for (cudaStream_t d : m.direct)

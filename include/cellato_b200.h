@@ -219,8 +219,12 @@ int cb2_checksum_planes(int automaton, const void* const* planes, int64_t x_size
  * traversers run one grid per launch sequence (traversers/cuda/simple.cuh:44-79);
  * cb2_batch_run_per_grid is that one-launch-per-grid path over the same grids
  * for comparison.  The grids stay owned by the caller; while they belong to a
- * batch, advance them through the batch (a grid advanced or re-uploaded
- * outside it makes the next cb2_batch_run rebuild the schedule). */
+ * batch, advance them through the batch (a grid advanced, re-uploaded,
+ * re-timed or re-seeded outside it makes the next cb2_batch_run rebuild the
+ * schedule).  Every registered automaton batches; a batch holding a lowered
+ * DSL automaton runs a kernel over all of them, in which each grid's draws,
+ * Margolus blocks and alternating algorithms follow its own generation and
+ * seed (cb2_grid_set_seed, cb2_grid_set_time_step). */
 typedef struct cb2_batch cb2_batch;
 
 typedef struct cb2_batch_opts {

@@ -120,10 +120,7 @@ def test_checksum_sums_state_values_not_indexes(ref):
     assert ck == want_ck
 
 
-def test_dsl_automata_outside_the_strip_kernels_are_refused(cuda):
-    with cb.DeviceGrid("brian", 64, 64) as g:
-        with pytest.raises(ValueError, match="batch kernel runs"):
-            cb.Batch([g], [10])
+def test_band_pass_without_time_refuses_dsl_automata(cuda):
     from cellato_b200 import _abi
     from cellato_b200.bands import BandGrid, _planes
     import ctypes
@@ -132,6 +129,68 @@ def test_dsl_automata_outside_the_strip_kernels_are_refused(cuda):
     rc = _abi.lib.cb2_band_pass(b.automaton, _planes(b.bufs[0]), _planes(b.bufs[1]), 256, b.rows_total,
                                 b.ghost, 64, 4, ctypes.byref(t), None)
     assert rc == _abi.CB2_EINVAL and "cb2_band_pass_at" in _abi.last_error()
+
+
+# narrow (exact-wrap row groups), ragged multi-strip, odd heights, tall
+BATCH_SHAPES = [(64, 48), (32 * 37, 61), (96, 7), (512, 40), (32 * 70, 37), (320, 130), (32, 3)]
+
+
+@pytest.mark.parametrize("opts", [{}, {"temporal_steps": 4, "tile_rows": 16}, {"temporal_steps": 2, "tile_rows": 9}])
+def test_batch_kernel_runs_dsl_automata(ref, opts):
+    # every lowered rule beside two networks in one batch, each grid with its own
+    # seed and length (remainder chunks); two runs, so the second continues the
+    # generations the device advanced after the first
+    rng = random.Random(len(opts))
+    names = DSL + ["game-of-life", "wire", "cyclic", "critters"]
+    cases = []
+    for i, name in enumerate(names):
+        x, y = BATCH_SHAPES[i % len(BATCH_SHAPES)]
+        # seeds within the reference's int run_params::seed
+        cases.append((name, x, y, rng.randrange(1, 40), rng.randrange(1, 1 << 31), cells_for(name, x, y, 100 + i)))
+    grids = []
+    for name, x, y, steps, seed, cells in cases:
+        g = cb.DeviceGrid(name, x, y)
+        g.upload_cells(cells)
+        g.set_seed(seed)
+        grids.append(g)
+    with cb.Batch(grids, [c[3] for c in cases], **opts) as b:
+        b.run()
+        b.wait()
+        b.run()
+        b.wait()
+    for g, (name, x, y, steps, seed, cells) in zip(grids, cases):
+        want, want_ck = ref.ref_run_named(name, cells, 2 * steps, seed=seed)
+        assert g.time_step == 2 * steps
+        assert (g.cells() == want).all(), (name, x, y, steps)
+        assert g.checksum_str() == want_ck, name
+        g.close()
+
+
+def test_batch_follows_time_and_seed_set_between_runs(ref):
+    # a grid re-timed and re-seeded between runs: the next run rebuilds the
+    # schedule and must equal the strip kernels from that generation and seed
+    names = ["lightning-forest", "critters", "traffic", "noisy-life"]
+    grids, cells0 = [], []
+    for i, name in enumerate(names):
+        c = cells_for(name, 160, 50, i)
+        g = cb.DeviceGrid(name, 160, 50)
+        g.upload_cells(c)
+        grids.append(g)
+        cells0.append(c)
+    with cb.Batch(grids, [13] * len(grids)) as b:
+        b.run()
+        b.wait()
+        mids = [g.cells() for g in grids]
+        for i, g in enumerate(grids):
+            g.time_step = 1000 + 7 * i
+            g.set_seed(99 + i)
+        b.run()
+        b.wait()
+    for i, (g, name) in enumerate(zip(grids, names)):
+        want, _ = device_run(name, mids[i], 13, seed=99 + i, time_step=1000 + 7 * i)
+        assert (g.cells() == want).all(), name
+        assert g.time_step == 1000 + 7 * i + 13
+        g.close()
 
 
 def test_served_dsl_requests(ref):
