@@ -151,46 +151,110 @@ __device__ __forceinline__ uint64_t sm_mix(uint64_t z) {
 }
 constexpr uint64_t kGolden = 0x9e3779b97f4a7c15ull;
 
-// Random 32-bit words for the lane's cells: the reference keys one 64-bit
-// stream per group of 64 cells and row; a 32-bit word takes its half.
+// The reference keys one 64-bit stream per (seed, stream, generation, group
+// of 64 cells, row): mix(mix(mix(mix(mix(seed + golden) ^ stream) ^ t) ^ x/64) ^ y).
+// All but the last mix are the same for every row of a level, so the strip
+// kernels compute this "lane key" once per task and level (ast_rule::init_keys).
+__device__ __forceinline__ uint64_t lane_key(uint64_t seed, uint64_t stream, int64_t t, int64_t xw) {
+    uint64_t k = sm_mix(seed + kGolden);
+    k = sm_mix(k ^ stream);
+    k = sm_mix(k ^ (uint64_t)t);
+    return sm_mix(k ^ (uint64_t)(xw >> 1));
+}
+
+// Random 32-bit words for the lane's cells: draw n of the row's stream is
+// mix(key + (n + 1) * golden), and a 32-bit word takes its half of it.
 struct word_stream {
     uint64_t key;
     uint64_t counter = 0;
     unsigned shift;
-    __device__ word_stream(const cell_ctx& c, uint64_t stream) : shift((unsigned)(c.xw & 1) * 32u) {
-        uint64_t k = sm_mix(c.seed + kGolden);
-        k = sm_mix(k ^ stream);
-        k = sm_mix(k ^ (uint64_t)c.t);
-        k = sm_mix(k ^ (uint64_t)(c.xw >> 1));
-        key = sm_mix(k ^ (uint64_t)c.y);
-    }
+    __device__ __forceinline__ word_stream(uint64_t lane, const cell_ctx& c)
+        : key(sm_mix(lane ^ (uint64_t)c.y)), shift((unsigned)(c.xw & 1) * 32u) {}
     __device__ __forceinline__ uint32_t next() {
         counter += kGolden;
         return (uint32_t)(sm_mix(key + counter) >> shift);
     }
 };
 
+// The same stream when this lane and lane^1 hold the two halves of one group
+// of 64 cells (cell_ctx::paired): the lane of the low half computes the even
+// draws, its partner the odd ones, and each sends the other the half it
+// uses -- one mix per two draws instead of one per draw.
+struct pair_stream {
+    uint64_t key;
+    uint64_t counter = 0;
+    unsigned shift;
+    __device__ __forceinline__ pair_stream(uint64_t lane, const cell_ctx& c)
+        : key(sm_mix(lane ^ (uint64_t)c.y)), shift((unsigned)(c.xw & 1) * 32u) {}
+    // Draws 2m and 2m+1 (this lane's halves); every lane of the warp calls it together.
+    __device__ __forceinline__ void next2(uint32_t& d0, uint32_t& d1) {
+        const bool high = shift != 0;
+        const uint64_t z = sm_mix(key + counter + (high ? 2 : 1) * kGolden);
+        counter += 2 * kGolden;
+        const uint32_t mine = (uint32_t)(z >> shift);
+        const uint32_t other = __shfl_xor_sync(kFullMask, (uint32_t)(z >> (32u - shift)), 1);
+        d0 = high ? other : mine;
+        d1 = high ? mine : other;
+    }
+};
+
 constexpr uint64_t gcd_of(uint64_t a, uint64_t b) { return b ? gcd_of(b, a % b) : a; }
 
-// Lane b is 1 with probability N/D (D a power of two): compares the binary
-// expansion of N/D with one fresh random digit per draw.
+// Draws the dyadic sampler below takes for N/D.
 template <uint64_t N, uint64_t D>
-__device__ __forceinline__ uint32_t dyadic_draw(word_stream& s) {
+constexpr int dyadic_draws() {
+    if constexpr (N == 0 || N == D)
+        return 0;
+    else if constexpr (N >= D - N)
+        return 1 + dyadic_draws<N - (D - N), D>();
+    else
+        return 1 + dyadic_draws<N + N, D>();
+}
+
+// Lane b is 1 with probability N/D (D a power of two): compares the binary
+// expansion of N/D with one fresh random digit per draw (draws[j] is digit j).
+template <uint64_t N, uint64_t D, int J = 0, int M>
+__device__ __forceinline__ uint32_t dyadic_draw(const uint32_t (&draws)[M]) {
     if constexpr (N == 0) {
         return 0u;
     } else if constexpr (N == D) {
         return 0xffffffffu;
     } else {
-        const uint32_t zero_bits = ~s.next();
+        const uint32_t zero_bits = ~draws[J];
         if constexpr (N >= D - N)
-            return zero_bits | dyadic_draw<N - (D - N), D>(s);
+            return zero_bits | dyadic_draw<N - (D - N), D, J + 1>(draws);
         else
-            return zero_bits & dyadic_draw<N + N, D>(s);
+            return zero_bits & dyadic_draw<N + N, D, J + 1>(draws);
+    }
+}
+
+// The threshold n/d in binary: after j digits the remainder is rem_after(j),
+// and digit j is 1 when 2 * rem >= d (compared before doubling, so that no
+// sum exceeds 2^64, as the reference does).
+constexpr uint64_t rem_after(uint64_t n, uint64_t d, int j) {
+    for (int i = 0; i < j; ++i) n = n >= d - n ? n - (d - n) : n + n;
+    return n;
+}
+
+// Digits J.. of the threshold against bits[J..]: a cell still active where its
+// random bit equals the digit; it turns 1 where the digit is 1 and its bit 0.
+// Inactive cells are left alone, so no per-lane test is needed.
+template <uint64_t n, uint64_t d, int J, int M>
+__device__ __forceinline__ void ratio_digits(const uint32_t (&bits)[M], uint32_t& active, uint32_t& result) {
+    if constexpr (J < M) {
+        constexpr uint64_t r = rem_after(n, d, J);
+        if constexpr (r >= d - r) {
+            result |= active & ~bits[J];
+            active &= bits[J];
+        } else {
+            active &= ~bits[J];
+        }
+        ratio_digits<n, d, J + 1>(bits, active, result);
     }
 }
 
 template <uint64_t Num, uint64_t Den>
-__device__ __forceinline__ uint32_t bernoulli_word(const cell_ctx& c, uint64_t stream) {
+__device__ __forceinline__ uint32_t bernoulli_word(const cell_ctx& c, uint64_t lane) {
     static_assert(Den > 0 && Num <= Den, "a probability lies in [0, 1]");
     if constexpr (Num == 0) {
         return 0u;
@@ -199,21 +263,28 @@ __device__ __forceinline__ uint32_t bernoulli_word(const cell_ctx& c, uint64_t s
     } else {
         constexpr uint64_t g = gcd_of(Num, Den);
         constexpr uint64_t n = Num / g, d = Den / g;
-        word_stream s(c, stream);
         if constexpr ((d & (d - 1)) == 0) {
-            return dyadic_draw<n, d>(s);
+            constexpr int M = dyadic_draws<n, d>();
+            uint32_t draws[M + (M & 1)];
+            if (c.paired) {  // warp-uniform
+                pair_stream s(lane, c);
+#pragma unroll
+                for (int j = 0; j < M; j += 2) s.next2(draws[j], draws[j + 1]);
+            } else {
+                word_stream s(lane, c);
+#pragma unroll
+                for (int j = 0; j < M; ++j) draws[j] = s.next();
+            }
+            return dyadic_draw<n, d>(draws);
         } else {
             // Recurring expansion: draw until every lane has left the threshold.
-            // The stream is counter-based, so the first kAhead draws are computed
-            // up front as independent instructions and consumed in order; draws
-            // past the one that resolves the last lane are simply not used.
-            constexpr int kAhead = 8;
-            uint32_t ahead[kAhead];
-#pragma unroll
-            for (int j = 0; j < kAhead; ++j) ahead[j] = s.next();
+            // The stream is counter-based, so the first draws are computed up front
+            // as independent instructions and compared with digits known at compile
+            // time; draws past the one that resolves the last lane are not used.
+            // A warp of 1024 cells needs about 11 digits, so a pair, whose shuffles
+            // make the tail dearer, computes 12 up front.
             uint32_t active = 0xffffffffu, result = 0;
-            uint64_t rem = n;
-            auto digit = [&](uint32_t bits) {
+            auto digit = [&](uint64_t& rem, uint32_t bits) {
                 if (rem >= d - rem) {
                     rem -= d - rem;
                     result |= active & ~bits;
@@ -223,14 +294,107 @@ __device__ __forceinline__ uint32_t bernoulli_word(const cell_ctx& c, uint64_t s
                     active &= ~bits;
                 }
             };
+            if (c.paired) {  // warp-uniform: the pair's shuffles run on every lane
+                constexpr int kAhead = 12;
+                uint32_t ahead[kAhead];
+                pair_stream s(lane, c);
 #pragma unroll
-            for (int j = 0; j < kAhead; ++j)
-                if (active) digit(ahead[j]);
-            while (active) digit(s.next());
+                for (int j = 0; j < kAhead; j += 2) s.next2(ahead[j], ahead[j + 1]);
+                ratio_digits<n, d, 0>(ahead, active, result);
+                uint64_t rem = rem_after(n, d, kAhead);
+                while (__any_sync(kFullMask, active)) {
+                    uint32_t d0, d1;
+                    s.next2(d0, d1);
+                    if (active) digit(rem, d0);
+                    if (active) digit(rem, d1);
+                }
+            } else {
+                constexpr int kAhead = 8;
+                uint32_t ahead[kAhead];
+                word_stream s(lane, c);
+#pragma unroll
+                for (int j = 0; j < kAhead; ++j) ahead[j] = s.next();
+                ratio_digits<n, d, 0>(ahead, active, result);
+                uint64_t rem = rem_after(n, d, kAhead);
+                while (active) digit(rem, s.next());
+            }
             return result;
         }
     }
 }
+
+// ---- the probability streams of a rule -----------------------------------------------------------
+// The distinct Stream values of the probability<N, D, Stream> nodes of an
+// AST, in order of first appearance: ast_rule keeps one lane key per stream
+// and level.
+template <uint64_t... S>
+struct stream_list {
+    static constexpr int size = sizeof...(S);
+};
+
+template <class L, uint64_t S>
+struct with_stream;
+template <uint64_t... T, uint64_t S>
+struct with_stream<stream_list<T...>, S> {
+    using type = std::conditional_t<((T == S) || ...), stream_list<T...>, stream_list<T..., S>>;
+};
+
+template <class L, class M>
+struct join_streams;
+template <class L>
+struct join_streams<L, stream_list<>> {
+    using type = L;
+};
+template <class L, uint64_t S, uint64_t... Rest>
+struct join_streams<L, stream_list<S, Rest...>> {
+    using type = typename join_streams<typename with_stream<L, S>::type, stream_list<Rest...>>::type;
+};
+
+template <class... Ls>
+struct join_all {
+    using type = stream_list<>;
+};
+template <class L, class... Ls>
+struct join_all<L, Ls...> {
+    using type = typename join_streams<L, typename join_all<Ls...>::type>::type;
+};
+
+template <class Node>
+struct streams_of {  // leaves: constants, neighbours, neighbourhood tags
+    using type = stream_list<>;
+};
+template <uint64_t Num, uint64_t Den, uint64_t S>
+struct streams_of<A::probability<Num, Den, S>> {
+    using type = stream_list<S>;
+};
+template <class V, int B>
+struct streams_of<A::has_bit_set<V, B>> {
+    using type = typename streams_of<V>::type;
+};
+template <template <class...> class T, class... Args>
+struct streams_of<T<Args...>> {
+    using type = typename join_all<typename streams_of<Args>::type...>::type;
+};
+
+template <uint64_t S, uint64_t... T>
+constexpr int slot_of(stream_list<T...>) {
+    constexpr uint64_t v[] = {T..., 0};
+    for (int i = 0; i < (int)sizeof...(T); ++i)
+        if (v[i] == S) return i;
+    return -1;
+}
+
+// A state dictionary that also names the rule's streams, so that the
+// probability evaluator finds its stream's slot in cell_ctx::key.
+template <class D, class Streams>
+struct keyed_dict : D {
+    using streams = Streams;
+};
+
+template <class D, class = void>
+struct has_streams : std::false_type {};
+template <class D>
+struct has_streams<D, std::void_t<typename D::streams>> : std::true_type {};
 
 // Lanes whose Margolus partner (in x) is the cell to their right, for
 // generation parity `odd`: even cells at even generations, odd cells at odd.
@@ -422,7 +586,15 @@ template <class Dict, uint64_t Num, uint64_t Den, uint64_t Stream>
 struct ev<Dict, A::probability<Num, Den, Stream>> {
     template <int P>
     __device__ __forceinline__ static bv<1> eval(const window<P>&, const cell_ctx& c) {
-        return mask(bernoulli_word<Num, Den>(c, Stream));
+        uint64_t lane;
+        if constexpr (has_streams<Dict>::value) {
+            constexpr int j = slot_of<Stream>(typename Dict::streams{});
+            static_assert(j >= 0, "stream missing from the rule's stream list");
+            lane = c.key ? c.key[j] : lane_key(c.seed, Stream, c.t, c.xw);
+        } else {
+            lane = lane_key(c.seed, Stream, c.t, c.xw);
+        }
+        return mask(bernoulli_word<Num, Den>(c, lane));
     }
 };
 
@@ -540,15 +712,31 @@ struct ev<Dict, A::margolus_180_neighbor> {
 template <class Config>
 struct ast_rule {
     using dict = typename Config::state_dictionary;
+    using streams = typename ast::streams_of<typename Config::algorithm>::type;
     static constexpr int P = dict::needed_bits;
     static constexpr int NH = 3 * P;  // (west, centre, east) word of each plane
     static constexpr bool kWindow = true;
+    static constexpr bool kDraws = streams::size > 0;  // the rule draws random numbers
+
+    // The lane keys of one level (cell_ctx::key), one per stream.
+    struct level_keys {
+        uint64_t k[streams::size > 0 ? streams::size : 1];
+    };
+    __device__ __forceinline__ static void init_keys(level_keys& keys, int64_t t, int64_t xw, uint64_t seed) {
+        init_keys(keys, t, xw, seed, streams{});
+    }
+    template <uint64_t... S>
+    __device__ __forceinline__ static void init_keys(level_keys& keys, int64_t t, int64_t xw, uint64_t seed,
+                                                     ast::stream_list<S...>) {
+        int j = 0;
+        ((keys.k[j++] = ast::lane_key(seed, S, t, xw)), ...);
+    }
 
     __device__ __forceinline__ static void next_at(const uint32_t (&a)[NH], const uint32_t (&m)[NH],
                                                    const uint32_t (&b)[NH], uint32_t (&o)[P],
                                                    const cell_ctx& c) {
         const ast::window<P> w{a, m, b};
-        const auto r = ast::ev<dict, typename Config::algorithm>::eval(w, c);
+        const auto r = ast::ev<ast::keyed_dict<dict, streams>, typename Config::algorithm>::eval(w, c);
         constexpr int N = sizeof(r.w) / 4;
 #pragma unroll
         for (int p = 0; p < P; ++p) o[p] = p < N ? r.w[p] : 0u;

@@ -39,8 +39,12 @@ __global__ void __launch_bounds__(32 * (K / L)) pipe_kernel(strip_launch a) {
     t.plane_words = a.plane_words;
     t.wd = a.wd;
     t.h = a.h;
-    t.x0 = sx * own;
-    t.nx = min(own, a.wd - t.x0);
+    // A rule that draws random numbers, one word per lane, on an even width:
+    // strips start at an odd column, so that the lanes pair up on groups of 64
+    // cells (the last strip owns column 0 through the wrap).
+    const int shift = draws_of<R>::value && V == 1 && (a.wd & 1) == 0 ? 1 : 0;
+    t.x0 = sx * own + shift;
+    t.nx = min(own, a.wd - sx * own);
     t.y0 = a.y_base + sy * a.tile_rows;
     t.ny = min(a.tile_rows, a.y_base + a.rows_out - t.y0);
     t.t0 = a.t0;

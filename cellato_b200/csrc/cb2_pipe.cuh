@@ -212,6 +212,22 @@ __device__ __forceinline__ void pipe_run_rows(const strip_task& t, const lane_ge
 #pragma unroll
                 for (int p = 0; p < P; ++p) s.c[g][q][i][p] = 0;
             }
+    // A stochastic rule keys its streams once per level (warp w's level g runs
+    // generation t0 + w*L + g for every row of the task), and with one word per
+    // lane, lanes 2m and 2m+1 holding the two halves of one group of 64 cells
+    // in one row split that group's draws (cell_ctx::paired).
+    bool paired = false;
+    if constexpr (draws_of<R>::value) {
+#pragma unroll
+        for (int g = 0; g < L; ++g)
+#pragma unroll
+            for (int i = 0; i < V; ++i) R::init_keys(s.keys[g][i], t.t0 + (int64_t)warp * L + g, geom.col[i], t.seed);
+        if constexpr (V == 1) {
+            const long long pc = __shfl_xor_sync(kFullMask, (long long)geom.col[0], 1);
+            const int py = __shfl_xor_sync(kFullMask, geom.yoff, 1);
+            paired = __all_sync(kFullMask, ((long long)geom.col[0] ^ 1) == pc && py == geom.yoff);
+        }
+    }
 
     uint32_t* ring = smem;
     uint32_t* hand = smem + DEPTH * SLOT;  // boundary b, parity q: hand + (2b + q) * RPS * SLOT
@@ -275,7 +291,7 @@ __device__ __forceinline__ void pipe_run_rows(const strip_task& t, const lane_ge
                 // output of the previous step, L rows behind its input)
                 // (a lane of a narrow grid's row group sweeps from its own first row)
                 row_ctx rc{t.t0 + (int64_t)warp * L, RPS * st + j - warp * (RPS + L), t.y0 + geom.yoff - K, t.h,
-                           t.seed, t.y_global0, t.global_h};
+                           t.seed, t.y_global0, t.global_h, paired};
                 strip_push<R, L, V, 0>(s, rows[j], geom.src_l, geom.src_r, &geom, &rc);
                 rc.sweep += 1;
                 strip_push<R, L, V, 1>(s, rows[j + 1], geom.src_l, geom.src_r, &geom, &rc);

@@ -27,6 +27,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 
 #include "cb2_rules.cuh"
 
@@ -49,12 +50,18 @@ struct strip_task {
 
 // Where a lane's 32 cells are, for rules that read it (window rules): the
 // generation the rule is evaluated at, the global row, the 32-bit word
-// column (cells 32*xw .. 32*xw+31) and the run's seed.
+// column (cells 32*xw .. 32*xw+31) and the run's seed.  Stochastic rules
+// also get the level's lane keys (their random streams keyed up to the
+// column, one per stream; null to key from scratch) and whether every lane
+// of the warp shares its group of 64 cells with lane^1 in the same row
+// (warp-uniform), in which case the pair splits the draws of that group.
 struct cell_ctx {
     int64_t t;
     int64_t y;
     int64_t xw;
     uint64_t seed;
+    const uint64_t* key = nullptr;
+    bool paired = false;
 };
 
 // Where a row pushed into a level chain sits: its sweep index (sweep row r is
@@ -68,6 +75,7 @@ struct row_ctx {
     uint64_t seed;
     int64_t y_global0;  // global row of row 0 of these planes
     int64_t global_h;   // rows of the whole grid
+    bool paired;        // cell_ctx::paired
 };
 
 constexpr unsigned kFullMask = 0xffffffffu;
@@ -124,10 +132,29 @@ __device__ __forceinline__ lane_geom<1> group_geom(const strip_task& t, int grou
     return g;
 }
 
+// Per-level lane keys of a window rule that draws random numbers
+// (R::level_keys); nothing for the other rules.
+struct no_keys {
+    static constexpr const uint64_t* k = nullptr;
+};
+template <class R, class = void>
+struct keys_of {
+    using type = no_keys;
+};
+template <class R>
+struct keys_of<R, std::void_t<typename R::level_keys>> {
+    using type = typename R::level_keys;
+};
+template <class R, class = void>
+struct draws_of : std::false_type {};
+template <class R>
+struct draws_of<R, std::void_t<decltype(R::kDraws)>> : std::bool_constant<R::kDraws> {};
+
 template <class R, int K, int V>
 struct strip_state {
     uint32_t h[K][2][V][R::NH];  // horizontal aggregates, slot = row parity
     uint32_t c[K][2][V][R::P];   // centre states, slot = row parity
+    typename keys_of<R>::type keys[K][V];
 };
 
 // One wavefront level: pushes `row` (a row of level g, parity slot Q) into
@@ -161,7 +188,7 @@ __device__ __forceinline__ void level_push(strip_state<R, K, V>& s, int g, uint3
         uint32_t nxt[V][P];
 #pragma unroll
         for (int i = 0; i < V; ++i) {
-            const cell_ctx c{rc->t + g, y, geom->col[i], rc->seed};
+            const cell_ctx c{rc->t + g, y, geom->col[i], rc->seed, s.keys[g][i].k, rc->paired};
             R::next_at(s.h[g][Q][i], s.h[g][1 - Q][i], hc[i], nxt[i], c);
         }
 #pragma unroll
