@@ -179,7 +179,9 @@ struct word_stream {
 // The same stream when this lane and lane^1 hold the two halves of one group
 // of 64 cells (cell_ctx::paired): the lane of the low half computes the even
 // draws, its partner the odd ones, and each sends the other the half it
-// uses -- one mix per two draws instead of one per draw.
+// uses -- one mix per two draws instead of one per draw.  (Letting a lone
+// lane draw both halves inside one shared path instead cost lightning-forest
+// a sixth of its speed: the second draw issues on every lane.)
 struct pair_stream {
     uint64_t key;
     uint64_t counter = 0;
@@ -190,9 +192,9 @@ struct pair_stream {
     __device__ __forceinline__ void next2(uint32_t& d0, uint32_t& d1) {
         const bool high = shift != 0;
         const uint64_t z = sm_mix(key + counter + (high ? 2 : 1) * kGolden);
-        counter += 2 * kGolden;
         const uint32_t mine = (uint32_t)(z >> shift);
         const uint32_t other = __shfl_xor_sync(kFullMask, (uint32_t)(z >> (32u - shift)), 1);
+        counter += 2 * kGolden;
         d0 = high ? other : mine;
         d1 = high ? mine : other;
     }

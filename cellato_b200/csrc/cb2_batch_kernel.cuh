@@ -140,10 +140,10 @@ __global__ void __launch_bounds__(kBatchWarps * 32) batch_kernel(batch_args a) {
             st.nx = gd.wd;
             geom = group_geom(st, task.groups, lane);
         } else {
-            // lowered rules on even widths: tiles start at an odd column, so that
-            // stochastic rules' lanes pair up on groups of 64 cells (the last tile
-            // owns column 0 through the wrap)
-            const int shift = D::kTimed && gd.automaton >= kNumBuiltin && (gd.wd & 1) == 0 ? 1 : 0;
+            // lowered rules: tiles start at an odd column, so that stochastic
+            // rules' lanes pair up on groups of 64 cells (the last tile owns
+            // column 0 through the wrap)
+            const int shift = D::kTimed && gd.automaton >= kNumBuiltin ? 1 : 0;
             st.x0 = task.tx * 30 + shift;
             st.nx = min(30, gd.wd - task.tx * 30);
             geom = strip_geom<1>(st, lane);

@@ -39,10 +39,11 @@ __global__ void __launch_bounds__(32 * (K / L)) pipe_kernel(strip_launch a) {
     t.plane_words = a.plane_words;
     t.wd = a.wd;
     t.h = a.h;
-    // A rule that draws random numbers, one word per lane, on an even width:
-    // strips start at an odd column, so that the lanes pair up on groups of 64
-    // cells (the last strip owns column 0 through the wrap).
-    const int shift = draws_of<R>::value && V == 1 && (a.wd & 1) == 0 ? 1 : 0;
+    // A rule that draws random numbers, one word per lane: strips start at an
+    // odd column, so that lanes 2m and 2m+1 hold the two halves of a group of
+    // 64 cells and split its draws (the last strip owns column 0 through the
+    // wrap; on an odd width the lanes past the wrap draw alone).
+    const int shift = draws_of<R>::value && V == 1 ? 1 : 0;
     t.x0 = sx * own + shift;
     t.nx = min(own, a.wd - sx * own);
     t.y0 = a.y_base + sy * a.tile_rows;

@@ -214,8 +214,10 @@ __device__ __forceinline__ void pipe_run_rows(const strip_task& t, const lane_ge
             }
     // A stochastic rule keys its streams once per level (warp w's level g runs
     // generation t0 + w*L + g for every row of the task), and with one word per
-    // lane, lanes 2m and 2m+1 holding the two halves of one group of 64 cells
-    // in one row split that group's draws (cell_ctx::paired).
+    // lane, lanes 2m and 2m+1 split the draws of a group of 64 cells when every
+    // pair of the warp holds the two halves of one group in one row
+    // (cell_ctx::paired; with strips starting at odd columns, all warps but
+    // those past the wrap of an odd width).
     bool paired = false;
     if constexpr (draws_of<R>::value) {
 #pragma unroll

@@ -10,7 +10,7 @@ side, traversers/cuda/temporal.hpp:44-59) and its height a multiple of the
 effective tile height, so it runs on the nearest smaller grid of that shape;
 the simple kernel and this project run on the exact bench size too.
 
-    python -m oracle.ref_cuda_bench [--quick] [--dsl]
+    python -m oracle.ref_cuda_bench [--quick] [--dsl] [--only NAME[,NAME...]]
 
 prints one JSON object per line (sweep points, then a summary per workload).
 With --dsl the workloads are the lowered DSL automata (every bundled
@@ -74,6 +74,7 @@ def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--quick", action="store_true", help="small grids, for a smoke check of the harness")
     ap.add_argument("--dsl", action="store_true", help="the lowered DSL automata instead of the headline three")
+    ap.add_argument("--only", default="", help="comma-separated workloads (automaton names) to run")
     args = ap.parse_args()
     import torch
 
@@ -88,6 +89,9 @@ def main() -> int:
             states = cb.automaton_info(n)[2]
             probs = [0.5, 0.25, 0.25] if states == 3 else [1.0 / states] * states  # exact binary fractions
             workloads.append((n, O.ref_automaton(n), 16384, 16384, probs, 42))
+    if args.only:
+        keep = set(args.only.split(","))
+        workloads = [w for w in workloads if w[0] in keep]
     for name, a, X, Y, probs, seed in workloads:
         if args.quick:
             X, Y = 30720, 1024  # a multiple of 32 and of 30 words
