@@ -87,7 +87,7 @@ struct batch_engine {
     batch_task* d_tasks = nullptr;
     batch_grid_desc* d_grids = nullptr;
     unsigned char* d_odd = nullptr;
-    unsigned* d_counters = nullptr;  // head, error, spare, ntasks
+    unsigned* d_counters = nullptr;  // head, error, ngrids (for the flip kernel), ntasks
     unsigned* d_task_done = nullptr; // per task
     batch_task* h_tasks = nullptr;   // pinned
     batch_grid_desc* h_grids = nullptr;
