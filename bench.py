@@ -261,9 +261,9 @@ def bench_batch(cb, torch, stream, n: int, runs: int, automata=(0, 1, 2)) -> dic
                     "(cb2_grid_run per grid)"}
 
 
-def serve_workload(n: int, seed: int = 7):
+def serve_workload(n: int, seed: int = 7, automata=(0, 1, 2)):
     """Requests: sides log-uniform in [128, 16384] (widths multiples of 32),
-    steps log-uniform in [1, 10000], automaton uniform, seeded inputs."""
+    steps log-uniform in [1, 10000], automaton uniform over `automata`, seeded inputs."""
     import numpy as np
 
     rng = np.random.default_rng(seed)
@@ -273,7 +273,7 @@ def serve_workload(n: int, seed: int = 7):
         x = int(min(16384, max(128, 32 * round(math.exp(rng.uniform(lo, hi)) / 32))))
         y = int(min(16384, max(128, round(math.exp(rng.uniform(lo, hi))))))
         steps = int(max(1, round(math.exp(rng.uniform(0.0, math.log(10000))))))
-        out.append((int(rng.integers(0, 3)), x, y, steps, 5000 + i))
+        out.append((automata[int(rng.integers(0, len(automata)))], x, y, steps, 5000 + i))
     return out
 
 
@@ -291,7 +291,7 @@ def serve_stream(cb, specs, rate: float, per_request: bool, seed: int = 11, **se
             due += gap
             while time.perf_counter() - t0 < due:
                 time.sleep(min(0.0005, max(0.0, due - (time.perf_counter() - t0))))
-            ids.append(srv.submit(a, x, y, steps, sd, BATCH_PROBS[a]))
+            ids.append(srv.submit(a, x, y, steps, sd, batch_probs(cb, a)))
         srv.drain(1200)
         st = [srv.status(i) for i in ids]
         stats = srv.stats()
@@ -304,8 +304,8 @@ def serve_stream(cb, specs, rate: float, per_request: bool, seed: int = 11, **se
             "server_plan_s": stats["plan_s"], "server_wait_s": stats["wait_s"], "batch_tasks": stats["tasks"]}
 
 
-def bench_serve(cb, n: int, rates) -> dict:
-    specs = serve_workload(n)
+def bench_serve(cb, n: int, rates, automata=(0, 1, 2)) -> dict:
+    specs = serve_workload(n, automata=automata)
     serve_stream(cb, specs[:20], 1000.0, False)  # warm-up: graph capture, pools
     serve_stream(cb, specs[:20], 1000.0, True)
     points = []
@@ -317,8 +317,9 @@ def bench_serve(cb, n: int, rates) -> dict:
         plain = serve_stream(cb, specs, rate, True)
         points.append({"rate_req_s": rate, "batched": batched, "per_request": plain,
                        "throughput_ratio": batched["throughput"] / plain["throughput"]})
+    names = ", ".join(cb.automaton_info(a)[0] if isinstance(a, int) else a for a in automata)
     return {"workload": f"{n} requests per rate, Poisson arrivals, sides log-uniform [128,16384] (widths multiple "
-                        "of 32), steps log-uniform [1,10000], automaton uniform, seeded inits",
+                        f"of 32), steps log-uniform [1,10000], automaton uniform {{{names}}}, seeded inits",
             "unit": METRIC, "latency": "submit to finished (checksum ready), ms",
             "memory_budget": "min(150 GiB, 80% of free device memory) of bit-plane state",
             "path": "cb2_server (continuous batching, persistent batch kernel per round) vs cb2_server per_request=1 "
@@ -352,6 +353,8 @@ def main() -> None:
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=300)
+    ap.add_argument("--serve-dsl-requests", type=int, default=300,
+                    help="requests of the served point over the lowered DSL automata (0 = skip)")
     ap.add_argument("--batch-grids", type=int, default=4096)
     ap.add_argument("--batch-dsl-grids", type=int, default=1024,
                     help="grids of the batched line over the lowered DSL automata (0 = skip)")
@@ -515,6 +518,9 @@ def main() -> None:
     served = None
     if not args.no_serve:
         served = bench_serve(cb, args.serve_requests, [100.0, 1000.0, 5000.0, 20000.0])
+    served_dsl = None
+    if not args.no_serve and args.serve_dsl_requests > 0 and all(n in cb.AUTOMATA for n in BATCH_DSL):
+        served_dsl = bench_serve(cb, args.serve_dsl_requests, [5000.0], automata=BATCH_DSL)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -547,6 +553,7 @@ def main() -> None:
         "batched": batched,
         "batched_dsl": batched_dsl,
         "served": served,
+        "served_dsl": served_dsl,
     }
     print(json.dumps(out), flush=True)
 

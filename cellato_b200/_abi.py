@@ -74,7 +74,7 @@ class ServerOpts(ctypes.Structure):
 class Request(ctypes.Structure):
     _fields_ = [("automaton", ctypes.c_int), ("x_size", ctypes.c_int64), ("y_size", ctypes.c_int64),
                 ("steps", ctypes.c_int64), ("seed", ctypes.c_uint64), ("n_thresholds", ctypes.c_int),
-                ("thresholds", ctypes.c_uint64 * 7), ("host_cells", ctypes.c_void_p),
+                ("thresholds", ctypes.c_uint64 * 31), ("host_cells", ctypes.c_void_p),
                 ("host_result", ctypes.c_void_p)]
 
 

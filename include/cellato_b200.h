@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define CB2_ABI_VERSION 2
+#define CB2_ABI_VERSION 3
 
 /* ---- status codes ------------------------------------------------------- */
 #define CB2_OK 0
@@ -283,7 +283,7 @@ typedef struct cb2_request {
     int64_t steps;
     uint64_t seed;          /* seeded input (cb2_grid_fill_random) when host_cells is NULL */
     int n_thresholds;
-    uint64_t thresholds[7];  /* at most 7 (the first 8 states of a larger dictionary) */
+    uint64_t thresholds[31]; /* at most states - 1 (31: every state of a 32-state dictionary) */
     const uint8_t* host_cells; /* optional input, one dictionary index per cell; read at
                                   admission, so it must stay valid until then            */
     uint8_t* host_result;      /* optional output, one index per cell, written at completion */

@@ -209,6 +209,28 @@ def test_served_dsl_requests(ref):
             assert (srv.result_cells(rid) == want).all(), name
 
 
+def test_served_seeded_requests_with_many_states(ref):
+    # device-seeded inputs over every state of a 32-state dictionary (31 thresholds in
+    # the request), batched with a 3-state stochastic rule: each equals the grid seeded
+    # and advanced alone
+    from fractions import Fraction
+    jobs = [("cyclic", 256, 96, 45, 77, [Fraction(1, 32)] * 32),
+            ("lightning-forest", 320, 70, 29, 78, [0.5, 0.25, 0.25]),
+            ("cyclic", 64, 40, 13, 79, [Fraction(1, 32)] * 32)]
+    with cb.Server(chunk_steps=16) as srv:
+        ids = [srv.submit(name, x, y, steps, seed, probs, want_cells=True) for (name, x, y, steps, seed, probs) in jobs]
+        srv.drain(120)
+        for rid, (name, x, y, steps, seed, probs) in zip(ids, jobs):
+            st = srv.wait(rid)
+            assert st["state"] == "done", st
+            with cb.DeviceGrid(name, x, y) as g:
+                g.fill_random(seed, probs)
+                cells = g.cells()
+            want, want_ck = ref.ref_run_named(name, cells, steps, seed=seed)
+            assert (srv.result_cells(rid) == want).all(), name
+            assert "-".join(str(v) for v in st["checksum"]) == want_ck, name
+
+
 def test_golden_fixtures(cuda):
     # committed outputs of the reference traverser: independent of oracle/_ref
     import json
