@@ -190,7 +190,7 @@ int batch_engine::build(const std::vector<batch_item>& items, const batch_tiling
             left -= k;
         }
         const int wd = g->g.wd, h = g->g.h;
-        const int rows = std::max(kmain, std::min(h, tiling.tile_rows));
+        const int rows = std::max(kmain, std::min(h, tiling.rows_for(g->g.automaton)));
         if (wd <= 16) {  // exact-wrap groups across the warp
             const int gmax = 32 / wd;
             p.rows = std::min(h, std::max((rows + gmax - 1) / gmax, 2 * kmain));
@@ -374,6 +374,7 @@ int cb2_batch_create(cb2_grid* const* grids, const int64_t* steps, int n, const 
     auto* b = new cb2_batch();
     b->tiling.temporal_steps = o.temporal_steps ? o.temporal_steps : 8;
     b->tiling.tile_rows = o.tile_rows > 0 ? o.tile_rows : 256;
+    b->tiling.lowered_tile_rows = o.tile_rows > 0 ? o.tile_rows : 64;
     int64_t est = 0;
     for (int i = 0; i < n; ++i) {
         if (!grids[i] || steps[i] < 0) {
@@ -383,7 +384,7 @@ int cb2_batch_create(cb2_grid* const* grids, const int64_t* steps, int n, const 
         b->items.push_back(batch_item{grids[i], steps[i], grids[i]->cur, grids[i]->time_step, grids[i]->seed});
         const cb2_grid* g = grids[i];
         const int64_t chunks = steps[i] / std::max(1, b->tiling.temporal_steps) + 4;
-        const int64_t rows = std::max<int64_t>(1, std::min<int64_t>(g->g.h, b->tiling.tile_rows));
+        const int64_t rows = std::max<int64_t>(1, std::min<int64_t>(g->g.h, b->tiling.rows_for(g->g.automaton)));
         const int64_t per_chunk =
             g->g.wd <= 16 ? (g->g.h + 1) / 2 + 1 : ((g->g.h + rows - 1) / rows) * ((g->g.wd + 29) / 30);
         est += chunks * per_chunk;

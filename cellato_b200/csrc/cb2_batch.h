@@ -61,7 +61,13 @@ struct batch_item {
 
 struct batch_tiling {
     int temporal_steps = 8;  // K of full chunks
-    int tile_rows = 256;     // output rows per strip task
+    int tile_rows = 256;     // output rows per strip task of a hand-written network
+    // ... of a lowered DSL rule.  Its tasks do ~100x the work per row, so with long
+    // tiles a long-running grid's chain of chunks, not the total work, sets the
+    // run's length (1024 mixed DSL grids: 1.87 Tcell/s at 256 rows, 2.19 at 128,
+    // 2.31 at 64, 2.02 at 32; the networks' mix is best at 256).
+    int lowered_tile_rows = 64;
+    int rows_for(int automaton) const { return automaton >= kNumBuiltin ? lowered_tile_rows : tile_rows; }
 };
 
 // The two kernels of a batch: the hand-written networks alone, or every

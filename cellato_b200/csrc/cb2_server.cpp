@@ -637,6 +637,7 @@ int cb2_server_create(const cb2_server_opts* opts, cb2_server** out) {
     if (m.opts.chunk_steps <= 0) m.opts.chunk_steps = 128;
     if (m.opts.max_active <= 0) m.opts.max_active = 4096;
     if (m.opts.temporal_steps <= 0) m.opts.temporal_steps = 8;
+    const bool tile_rows_given = m.opts.tile_rows > 0;
     if (m.opts.tile_rows <= 0) m.opts.tile_rows = 128;
     if (m.opts.task_capacity <= 0) m.opts.task_capacity = 1 << 20;
     // Measured on the served mix (sides up to 16384): with 128-generation
@@ -645,6 +646,7 @@ int cb2_server_create(const cb2_server_opts* opts, cb2_server** out) {
     if (m.opts.direct_cells == 0) m.opts.direct_cells = 1ll << 28;
     m.tiling.temporal_steps = m.opts.temporal_steps;
     m.tiling.tile_rows = m.opts.tile_rows;
+    m.tiling.lowered_tile_rows = tile_rows_given ? m.opts.tile_rows : 64;
     m.t0 = clock_t_::now();
     cudaGetDevice(&m.device);
     size_t free_b = 0, total_b = 0;

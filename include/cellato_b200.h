@@ -229,7 +229,8 @@ typedef struct cb2_batch cb2_batch;
 
 typedef struct cb2_batch_opts {
     int temporal_steps;   /* K of full chunks: 1, 2, 4 or 8 (0 = 8)                  */
-    int tile_rows;        /* output rows per strip task (0 = 256)                      */
+    int tile_rows;        /* output rows per strip task (0 = 256 for the hand-written
+                             networks, 64 for lowered DSL rules)                       */
     long long spin_limit; /* iterations a task waits for its grid's previous chunk
                              before the run fails with CB2_ETIMEOUT (0 = ~4 s)         */
     int stall_task;       /* test hook: index of a task whose dependency is never
@@ -264,7 +265,8 @@ typedef struct cb2_server_opts {
     int max_active;          /* requests admitted at once (0 = 4096)                    */
     int chunk_steps;         /* most generations per request per round (0 = 128)       */
     int temporal_steps;      /* K of the batch kernel: 1, 2, 4 or 8 (0 = 8)            */
-    int tile_rows;           /* output rows per strip task (0 = 128)                   */
+    int tile_rows;           /* output rows per strip task (0 = 128 for the hand-written
+                                networks, 64 for lowered DSL rules)                    */
     int per_request;         /* 1 = plain one-request-at-a-time path                   */
     int task_capacity;       /* strip tasks per round (0 = 2^20)                        */
     long long spin_limit;    /* bounded wait of a task (0 = ~4 s)                       */
