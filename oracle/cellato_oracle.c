@@ -8,7 +8,9 @@
  *
  * Parity pin: every function here is checked against the reference itself,
  * compiled from its own headers into oracle/_ref/ (ref_shim.cpp), and against
- * the committed golden fixtures generated from that build (tests/golden/).
+ * the committed golden fixtures generated from that build (tests/golden/);
+ * the probability sampler (orc_sample_ratio) against the reference's own
+ * scripted-word known answers (tests/probability.hpp:69-110).
  *
  * Cell encoding: one uint8 per cell holding the state-dictionary index
  * (memory/state_dictionary.hpp:10-42).  For the three bundled automata used
@@ -364,4 +366,70 @@ int orc_unpack_tiled(const uint8_t* in, int64_t X, int64_t Y, int P, int W, uint
             cells[y * X + x] = s;
         }
     return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Exact Bernoulli(num/den) sampling of probability<N, D, S>                 */
+/* (core/probability.hpp:27-87).  Lane b of the result is 1 with             */
+/* probability num/den; digit j of the comparison is bit b of words[j].      */
+/* A power-of-two denominator compares its finite binary expansion with one  */
+/* fresh word per digit (sample_dyadic, :27-43); any other ratio draws until */
+/* every active lane has left the threshold (sample_ratio, :45-87), so no    */
+/* precision is fixed.  Lanes outside `active` are never set.  lane_bits is  */
+/* the word width (8, 16, 32 or 64); *used returns the words consumed, or -1 */
+/* when `words` ran out first.                                               */
+/* ------------------------------------------------------------------------ */
+static uint64_t orc_gcd(uint64_t a, uint64_t b) {
+    while (b) {
+        uint64_t r = a % b;
+        a = b;
+        b = r;
+    }
+    return a;
+}
+
+static uint64_t orc_dyadic(uint64_t num, uint64_t den, const uint64_t* words, int nwords, uint64_t mask, int* used) {
+    if (num == 0) return 0;
+    if (num == den) return mask;
+    if (*used < 0 || *used >= nwords) {
+        *used = -1;
+        return 0;
+    }
+    const uint64_t zero_bits = ~words[(*used)++] & mask;
+    if (num >= den - num) return zero_bits | orc_dyadic(num - (den - num), den, words, nwords, mask, used);
+    return zero_bits & orc_dyadic(num + num, den, words, nwords, mask, used);
+}
+
+uint64_t orc_sample_ratio(uint64_t num, uint64_t den, const uint64_t* words, int nwords, uint64_t active,
+                          int lane_bits, int* used) {
+    const uint64_t mask = lane_bits >= 64 ? ~0ull : ((1ull << lane_bits) - 1);
+    *used = 0;
+    active &= mask;
+    if (den == 0 || num > den) {
+        *used = -1;
+        return 0;
+    }
+    if (num == 0) return 0;
+    if (num == den) return active;
+    const uint64_t g = orc_gcd(num, den);
+    const uint64_t n = num / g, d = den / g;
+    if (active == 0) return 0;
+    if ((d & (d - 1)) == 0) return active & orc_dyadic(n, d, words, nwords, mask, used);
+    uint64_t result = 0, rem = n;
+    while (active) {
+        if (*used >= nwords) {
+            *used = -1;
+            return result;
+        }
+        const uint64_t bits = words[(*used)++] & mask;
+        if (rem >= d - rem) { /* digit 1, compared before doubling: no overflow */
+            rem -= d - rem;
+            result |= active & ~bits;
+            active &= bits;
+        } else {
+            rem += rem;
+            active &= ~bits;
+        }
+    }
+    return result;
 }

@@ -60,8 +60,23 @@ def _lib():
             getattr(lib, name).argtypes = [_u8p, _i64, _i64, ctypes.c_int, _u8p]
         for name in ("orc_pack_bit_array", "orc_unpack_bit_array", "orc_pack_tiled", "orc_unpack_tiled"):
             getattr(lib, name).argtypes = [_u8p, _i64, _i64, ctypes.c_int, ctypes.c_int, _u8p]
+        lib.orc_sample_ratio.argtypes = [ctypes.c_uint64, ctypes.c_uint64, _u64p, ctypes.c_int, ctypes.c_uint64,
+                                         ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        lib.orc_sample_ratio.restype = ctypes.c_uint64
         _oracle = lib
     return _oracle
+
+
+def sample_ratio(num: int, den: int, words, active: int | None = None, lane_bits: int = 64) -> tuple[int, int]:
+    """Exact Bernoulli(num/den) per lane from scripted random words (digit j =
+    words[j]), as core/probability.hpp:27-87; returns (lanes set, words used),
+    words used = -1 when the words ran out."""
+    w = np.ascontiguousarray(np.array([int(v) for v in words] or [0], dtype=np.uint64))
+    used = ctypes.c_int()
+    mask = (1 << lane_bits) - 1
+    r = _lib().orc_sample_ratio(num, den, _p(w, _u64p), len(words), mask if active is None else active, lane_bits,
+                                ctypes.byref(used))
+    return int(r), used.value
 
 
 def ref_available() -> bool:

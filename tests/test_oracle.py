@@ -84,3 +84,47 @@ def test_thresholds_accept_decimal_probabilities_that_sum_to_one_within_rounding
     assert list(exact) == [(1 << 53) // 3, (2 << 53) // 3]
     with pytest.raises(ValueError):
         O.thresholds([0.5, 0.4])
+
+
+def test_sample_ratio_matches_the_reference_known_answers():
+    # The scripted-word known answers of the reference's own tests
+    # (tests/probability.hpp:69-110), run through the oracle's restatement of
+    # sample_dyadic / sample_ratio (core/probability.hpp:27-87).
+    S = O.sample_ratio
+    assert S(0, 3, [], lane_bits=8) == (0, 0)            # probability zero clears every lane
+    assert S(3, 3, [], lane_bits=8) == (0xFF, 0)         # probability one sets every lane
+    assert S(3, 3, [], active=0x25, lane_bits=8) == (0x25, 0)
+    assert S(1, 3, [], active=0, lane_bits=8) == (0, 0)  # no active lanes need no random bits
+    # lane k represents k/8, most significant digit drawn first
+    assert S(1, 2, [0xF0], lane_bits=8) == (0x0F, 1)
+    assert S(1, 4, [0xF0, 0xCC], lane_bits=8) == (0x03, 2)
+    assert S(3, 8, [0xF0, 0xCC, 0xAA], lane_bits=8) == (0x07, 3)
+    assert S(1, 3, [0xF0, 0xCC, 0xAA, 0, 0], lane_bits=8)[0] == 0x07
+    assert S(2, 3, [0xF0, 0xCC, 0xAA, 0, 0], lane_bits=8)[0] == 0x3F
+    assert S(3, 8, [0xF0, 0xCC, 0xAA], active=0x55, lane_bits=8)[0] == 0x05  # never sets inactive lanes
+    # 1/3 = 0.010101...: 101 matching digits, then a smaller one; no truncation at 64 digits
+    ones = (1 << 64) - 1
+    prefix = [ones if d % 2 == 0 else 0 for d in range(1, 102)] + [0]
+    assert S(1, 3, prefix) == (ones, 102)
+    # extreme numerators and denominators do not overflow
+    assert S(1, ones, [0] * 64)[0] == ones
+    assert S(ones - 1, ones, [ones] * 64)[0] == 0
+
+
+def test_sample_ratio_frequencies_and_reduction():
+    # Reduced and unreduced ratios agree word for word, and the lanes set by
+    # random words approach the probability (the reference's frequency check,
+    # tests/probability.hpp:112-140, on the restatement).
+    rng = np.random.default_rng(3)
+    words = [int(w) for w in rng.integers(0, np.iinfo(np.uint64).max, 4000, dtype=np.uint64, endpoint=True)]
+    for num, den in [(1, 3), (3, 100), (1, 1000), (3, 4), (5, 8)]:
+        assert O.sample_ratio(num, den, words[:200]) == O.sample_ratio(num * 7, den * 7, words[:200])
+        hits, pos = 0, 0
+        for _ in range(200):
+            r, used = O.sample_ratio(num, den, words[pos:pos + 80])
+            assert used > 0
+            hits += bin(r).count("1")
+            pos = (pos + used) % 3900
+        freq = hits / (200 * 64)
+        sd = (num / den * (1 - num / den) / (200 * 64)) ** 0.5
+        assert abs(freq - num / den) < 6 * sd + 1e-4, (num, den, freq)
