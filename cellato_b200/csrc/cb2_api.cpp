@@ -119,9 +119,26 @@ static const int kDefaultPlan[kNumBuiltin][4] = {{32, 2, 16, 4}, {32, 1, 16, 4},
 // Lowered DSL automata: a window of 3P words per row and level keeps the
 // register count in check only for short chains.
 static const int kDefaultDslPlan[4] = {8, 1, 2, 2};
+// The bundled lowered automata and the two stochastic examples: the plans
+// cb2_autotune picked for each at 16384^2 with uniform states (the lighter
+// rules go deeper; the Margolus, stochastic and 32-state ones stay short).
+struct named_plan {
+    const char* name;
+    int plan[4];
+};
+static const named_plan kMeasuredDslPlans[] = {
+    {"brian", {16, 1, 4, 2}},    {"forest-fire", {16, 1, 4, 2}}, {"fluid", {16, 1, 4, 2}},
+    {"maze", {16, 1, 4, 2}},     {"traffic", {16, 1, 4, 2}},     {"critters", {8, 2, 2, 2}},
+    {"noisy-life", {8, 2, 2, 2}}, {"cyclic", {8, 1, 4, 2}},      {"lightning-forest", {4, 1, 1, 2}},
+};
 
 static const int* default_plan(int automaton) {
-    return automaton < kNumBuiltin ? kDefaultPlan[automaton] : kDefaultDslPlan;
+    if (automaton < kNumBuiltin) return kDefaultPlan[automaton];
+    const char* name = name_of(automaton);
+    for (const named_plan& p : kMeasuredDslPlans)
+        if (name && std::strcmp(name, p.name) == 0 && find_variant(automaton, p.plan[0], p.plan[1], p.plan[2], p.plan[3]))
+            return p.plan;
+    return kDefaultDslPlan;
 }
 
 // Fills every 0 field of `t` for a grid of geometry g.

@@ -219,6 +219,30 @@ __device__ __forceinline__ void pipe_run_rows(const strip_task& t, const lane_ge
     // (cell_ctx::paired; with strips starting at odd columns, all warps but
     // those past the wrap of an odd width).
     bool paired = false;
+    // The global row each pushed row's first level outputs, kept as running
+    // local (these planes, wrap at t.h) and global (wrap at the grid's rows)
+    // counters: no division per row.  The first row pushed (sweep
+    // -warp*(RPS+L), possibly a warm-up row of a later warp) outputs local row
+    // y0 + yoff - K - 1 + sweep; a local wrap resyncs the global row to the
+    // planes' offset.  Levels map their rows in global rows (row_ctx): a band's
+    // local wrap only happens in rows no output depends on, since its ghost
+    // rows are at least K deep.
+    int64_t ylocal = 0, yglob = 0, yshift = 0, gh = 1;
+    if constexpr (R::kWindow) {
+        gh = t.global_h;
+        const int64_t s0 = (int64_t)t.y0 + geom.yoff - K - 1 - (int64_t)warp * (RPS + L);
+        ylocal = ((s0 % t.h) + t.h) % t.h;
+        yshift = ((t.y_global0 % gh) + gh) % gh;
+        yglob = (ylocal + yshift) % gh;
+    }
+    auto next_row = [&]() {
+        if (++ylocal == t.h) {
+            ylocal = 0;
+            yglob = yshift;
+        } else if (++yglob == gh) {
+            yglob = 0;
+        }
+    };
     if constexpr (draws_of<R>::value) {
 #pragma unroll
         for (int g = 0; g < L; ++g)
@@ -290,12 +314,13 @@ __device__ __forceinline__ void pipe_run_rows(const strip_task& t, const lane_ge
         for (int j = 0; j < RPS; j += 2) {
             if constexpr (R::kWindow) {
                 // warp w's chain receives sweep row RPS*st + j - w*(RPS + L) (warp w-1's
-                // output of the previous step, L rows behind its input)
-                // (a lane of a narrow grid's row group sweeps from its own first row)
-                row_ctx rc{t.t0 + (int64_t)warp * L, RPS * st + j - warp * (RPS + L), t.y0 + geom.yoff - K, t.h,
-                           t.seed, t.y_global0, t.global_h, paired};
+                // output of the previous step, L rows behind its input); a lane of a
+                // narrow grid's row group sweeps from its own first row
+                row_ctx rc{t.t0 + (int64_t)warp * L, yglob, gh, t.seed, paired};
+                next_row();
                 strip_push<R, L, V, 0>(s, rows[j], geom.src_l, geom.src_r, &geom, &rc);
-                rc.sweep += 1;
+                rc.y = yglob;
+                next_row();
                 strip_push<R, L, V, 1>(s, rows[j + 1], geom.src_l, geom.src_r, &geom, &rc);
             } else {
                 strip_push<R, L, V, 0>(s, rows[j], geom.src_l, geom.src_r);

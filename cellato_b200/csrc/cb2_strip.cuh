@@ -64,18 +64,16 @@ struct cell_ctx {
     bool paired = false;
 };
 
-// Where a row pushed into a level chain sits: its sweep index (sweep row r is
-// grid row y0 - K + r, mod h) and the generation of the chain's first level.
-// Only window rules (ast_rule) read it.
+// Where a row pushed into a level chain sits, for window rules (ast_rule):
+// the generation of the chain's first level and the global row that level
+// outputs (the row above its input); level g outputs the row g above that,
+// modulo the grid's rows.
 struct row_ctx {
-    int64_t t;     // generation of the first level of the chain
-    int sweep;     // sweep index of the row entering the first level
-    int y_base;    // row of sweep index 0 in these planes (y0 - K)
-    int h;         // rows of these planes
+    int64_t t;   // generation of the first level of the chain
+    int64_t y;   // global row of the first level's output, 0 <= y < gh
+    int64_t gh;  // rows of the whole grid
     uint64_t seed;
-    int64_t y_global0;  // global row of row 0 of these planes
-    int64_t global_h;   // rows of the whole grid
-    bool paired;        // cell_ctx::paired
+    bool paired;  // cell_ctx::paired
 };
 
 constexpr unsigned kFullMask = 0xffffffffu;
@@ -181,10 +179,10 @@ __device__ __forceinline__ void level_push(strip_state<R, K, V>& s, int g, uint3
                 hc[i][3 * p + 2] = east_of(row[i][p], r);
             }
         }
-        // level g outputs the row one above its input: sweep index rc->sweep - g - 1
-        int64_t y = ((int64_t)rc->y_base + rc->sweep - g - 1) % rc->h;
-        if (y < 0) y += rc->h;
-        y = (y + rc->y_global0) % rc->global_h;  // a band's rows are global rows y_global0..
+        // level g outputs the row g above the first level's (no division: one
+        // add in all but grids of fewer rows than levels)
+        int64_t y = rc->y - g;
+        while (y < 0) y += rc->gh;
         uint32_t nxt[V][P];
 #pragma unroll
         for (int i = 0; i < V; ++i) {
