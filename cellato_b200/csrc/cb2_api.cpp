@@ -120,8 +120,8 @@ static const int kDefaultPlan[kNumBuiltin][4] = {{32, 2, 16, 4}, {32, 1, 16, 4},
 // register count in check only for short chains.
 static const int kDefaultDslPlan[4] = {8, 1, 2, 2};
 // The bundled lowered automata and the two stochastic examples: the plans
-// cb2_autotune picked for each at 16384^2 with uniform states (the lighter
-// rules go deeper; the Margolus, stochastic and 32-state ones stay short).
+// cb2_autotune picked for each at 16384^2 with uniform states (most go
+// sixteen levels deep; the Margolus, two-draw and 32-state ones stay short).
 struct named_plan {
     const char* name;
     int plan[4];
@@ -129,7 +129,7 @@ struct named_plan {
 static const named_plan kMeasuredDslPlans[] = {
     {"brian", {16, 1, 4, 2}},    {"forest-fire", {16, 1, 4, 2}}, {"fluid", {16, 1, 4, 2}},
     {"maze", {16, 1, 4, 2}},     {"traffic", {16, 1, 4, 2}},     {"critters", {8, 2, 2, 2}},
-    {"noisy-life", {8, 2, 2, 2}}, {"cyclic", {8, 1, 4, 2}},      {"lightning-forest", {4, 1, 1, 2}},
+    {"noisy-life", {16, 1, 4, 2}}, {"cyclic", {8, 1, 4, 2}},     {"lightning-forest", {4, 1, 1, 2}},
 };
 
 static const int* default_plan(int automaton) {

@@ -234,14 +234,15 @@ __device__ __forceinline__ void pipe_run_rows(const strip_task& t, const lane_ge
         ylocal = ((s0 % t.h) + t.h) % t.h;
         yshift = ((t.y_global0 % gh) + gh) % gh;
         yglob = (ylocal + yshift) % gh;
+#pragma unroll
+        for (int g = 0; g < L; ++g) s.rows.gm[g] = g % gh;
     }
+    // branch-free, like the row pushes around it (a branch splits their code)
     auto next_row = [&]() {
-        if (++ylocal == t.h) {
-            ylocal = 0;
-            yglob = yshift;
-        } else if (++yglob == gh) {
-            yglob = 0;
-        }
+        const bool wrap = ylocal + 1 == t.h;
+        ylocal = wrap ? 0 : ylocal + 1;
+        const int64_t yn = yglob + 1 == gh ? 0 : yglob + 1;
+        yglob = wrap ? yshift : yn;
     };
     if constexpr (draws_of<R>::value) {
 #pragma unroll

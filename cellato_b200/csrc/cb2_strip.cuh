@@ -148,11 +148,21 @@ struct draws_of : std::false_type {};
 template <class R>
 struct draws_of<R, std::void_t<decltype(R::kDraws)>> : std::bool_constant<R::kDraws> {};
 
+// Per-level row offsets of a window rule: level g outputs the row g above
+// the first level's, and gm[g] = g mod (the grid's rows), so that one
+// conditional add wraps it; nothing for the other rules.
+template <int K>
+struct level_rows {
+    int64_t gm[K];
+};
+struct no_level_rows {};
+
 template <class R, int K, int V>
 struct strip_state {
     uint32_t h[K][2][V][R::NH];  // horizontal aggregates, slot = row parity
     uint32_t c[K][2][V][R::P];   // centre states, slot = row parity
     typename keys_of<R>::type keys[K][V];
+    std::conditional_t<R::kWindow, level_rows<K>, no_level_rows> rows;
 };
 
 // One wavefront level: pushes `row` (a row of level g, parity slot Q) into
@@ -179,10 +189,10 @@ __device__ __forceinline__ void level_push(strip_state<R, K, V>& s, int g, uint3
                 hc[i][3 * p + 2] = east_of(row[i][p], r);
             }
         }
-        // level g outputs the row g above the first level's (no division: one
-        // add in all but grids of fewer rows than levels)
-        int64_t y = rc->y - g;
-        while (y < 0) y += rc->gh;
+        // level g outputs the row g above the first level's: no division and no
+        // branch, which would split the unrolled levels' code
+        int64_t y = rc->y - s.rows.gm[g];
+        y = y < 0 ? y + rc->gh : y;
         uint32_t nxt[V][P];
 #pragma unroll
         for (int i = 0; i < V; ++i) {
