@@ -289,56 +289,73 @@ __device__ __forceinline__ void pipe_run_rows(const strip_task& t, const lane_ge
     }
     __syncthreads();
 
-    for (int st = 0; st < steps; ++st) {
-        uint32_t rows[RPS][V][P];
-        if (warp == 0) {
-            issue(st + G - 1);
-            cp_async_wait<G - 1>();
+    // The rows, with the generation of this warp's first level.  A rule that
+    // branches on the generation's parity (alternate_algorithms) gets one copy
+    // of the loop per parity of the task's first generation, chosen once per
+    // CTA: with an even number of levels per warp every level's parity is then
+    // a compile-time constant and the branch folds.
+    auto sweep = [&](auto parity) {
+        constexpr int PAR = decltype(parity)::value;
+        const int64_t tbase = (PAR < 0 ? t.t0 : ((t.t0 & ~(int64_t)1) | PAR)) + (int64_t)warp * L;
+        for (int st = 0; st < steps; ++st) {
+            uint32_t rows[RPS][V][P];
+            if (warp == 0) {
+                issue(st + G - 1);
+                cp_async_wait<G - 1>();
 #pragma unroll
-            for (int j = 0; j < RPS; ++j) {
-                const int r = RPS * st + j;
-                if (r < total) {
-                    slot_read<R, V>(ring + (r % DEPTH) * SLOT, lane, rows[j]);
+                for (int j = 0; j < RPS; ++j) {
+                    const int r = RPS * st + j;
+                    if (r < total) {
+                        slot_read<R, V>(ring + (r % DEPTH) * SLOT, lane, rows[j]);
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < V; ++i)
+#pragma unroll
+                            for (int p = 0; p < P; ++p) rows[j][i][p] = 0;
+                    }
+                }
+            } else {
+                const uint32_t* in = hand + ((warp - 1) * 2 + (st & 1)) * RPS * SLOT;
+#pragma unroll
+                for (int j = 0; j < RPS; ++j) slot_read<R, V>(in + j * SLOT, lane, rows[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < RPS; j += 2) {
+                if constexpr (R::kWindow) {
+                    // warp w's chain receives sweep row RPS*st + j - w*(RPS + L) (warp w-1's
+                    // output of the previous step, L rows behind its input); a lane of a
+                    // narrow grid's row group sweeps from its own first row
+                    row_ctx rc{tbase, yglob, gh, t.seed, paired};
+                    next_row();
+                    strip_push<R, L, V, 0>(s, rows[j], geom.src_l, geom.src_r, &geom, &rc);
+                    rc.y = yglob;
+                    next_row();
+                    strip_push<R, L, V, 1>(s, rows[j + 1], geom.src_l, geom.src_r, &geom, &rc);
                 } else {
-#pragma unroll
-                    for (int i = 0; i < V; ++i)
-#pragma unroll
-                        for (int p = 0; p < P; ++p) rows[j][i][p] = 0;
+                    strip_push<R, L, V, 0>(s, rows[j], geom.src_l, geom.src_r);
+                    strip_push<R, L, V, 1>(s, rows[j + 1], geom.src_l, geom.src_r);
                 }
             }
-        } else {
-            const uint32_t* in = hand + ((warp - 1) * 2 + (st & 1)) * RPS * SLOT;
+            if (warp == W - 1) {
+                const int r0 = RPS * (st - (W - 1));  // input rows whose results leave now
 #pragma unroll
-            for (int j = 0; j < RPS; ++j) slot_read<R, V>(in + j * SLOT, lane, rows[j]);
-        }
-#pragma unroll
-        for (int j = 0; j < RPS; j += 2) {
-            if constexpr (R::kWindow) {
-                // warp w's chain receives sweep row RPS*st + j - w*(RPS + L) (warp w-1's
-                // output of the previous step, L rows behind its input); a lane of a
-                // narrow grid's row group sweeps from its own first row
-                row_ctx rc{t.t0 + (int64_t)warp * L, yglob, gh, t.seed, paired};
-                next_row();
-                strip_push<R, L, V, 0>(s, rows[j], geom.src_l, geom.src_r, &geom, &rc);
-                rc.y = yglob;
-                next_row();
-                strip_push<R, L, V, 1>(s, rows[j + 1], geom.src_l, geom.src_r, &geom, &rc);
+                for (int j = 0; j < RPS; ++j)
+                    if (r0 + j >= 2 * K && r0 + j < total) strip_store<R, V>(t, geom, r0 + j - 2 * K, rows[j]);
             } else {
-                strip_push<R, L, V, 0>(s, rows[j], geom.src_l, geom.src_r);
-                strip_push<R, L, V, 1>(s, rows[j + 1], geom.src_l, geom.src_r);
+                uint32_t* out = hand + (warp * 2 + ((st + 1) & 1)) * RPS * SLOT;
+#pragma unroll
+                for (int j = 0; j < RPS; ++j) slot_write<R, V>(out + j * SLOT, lane, rows[j]);
             }
+            __syncthreads();
         }
-        if (warp == W - 1) {
-            const int r0 = RPS * (st - (W - 1));  // input rows whose results leave now
-#pragma unroll
-            for (int j = 0; j < RPS; ++j)
-                if (r0 + j >= 2 * K && r0 + j < total) strip_store<R, V>(t, geom, r0 + j - 2 * K, rows[j]);
-        } else {
-            uint32_t* out = hand + (warp * 2 + ((st + 1) & 1)) * RPS * SLOT;
-#pragma unroll
-            for (int j = 0; j < RPS; ++j) slot_write<R, V>(out + j * SLOT, lane, rows[j]);
-        }
-        __syncthreads();
+    };
+    if constexpr (parity_of<R>::value && L % 2 == 0) {
+        if (t.t0 & 1)  // the same for every warp of the CTA: the barriers in sweep stay uniform
+            sweep(std::integral_constant<int, 1>{});
+        else
+            sweep(std::integral_constant<int, 0>{});
+    } else {
+        sweep(std::integral_constant<int, -1>{});
     }
     if (warp == 0) cp_async_wait<0>();
 }

@@ -147,6 +147,11 @@ template <class R, class = void>
 struct draws_of : std::false_type {};
 template <class R>
 struct draws_of<R, std::void_t<decltype(R::kDraws)>> : std::bool_constant<R::kDraws> {};
+// Window rules that branch on the parity of the generation (R::kParity).
+template <class R, class = void>
+struct parity_of : std::false_type {};
+template <class R>
+struct parity_of<R, std::void_t<decltype(R::kParity)>> : std::bool_constant<R::kParity> {};
 
 // Per-level row offsets of a window rule: level g outputs the row g above
 // the first level's, and gm[g] = g mod (the grid's rows), so that one
