@@ -65,7 +65,7 @@
 namespace cb2 {
 
 constexpr int kBuiltinPlanes = 3;  // the hand-written networks' largest P
-constexpr int kBuiltinRows = 4;    // rows each warp passes on per barrier (2: 18.3, 4: 19.1 Tcell/s)
+constexpr int kBuiltinRows = 4;    // rows each warp passes on per barrier (2: 18.3, 4: 19.1, 8: 16.6 Tcell/s)
 
 // The hand-written networks: the kernel of kind kBatchBuiltin.  KMAX = 4
 // drops the eight-generation pipelines (a batch whose chunks are at most 4).

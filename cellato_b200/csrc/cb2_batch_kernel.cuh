@@ -19,10 +19,13 @@ namespace cb2 {
 constexpr int kBatchWarps = 4;  // warps of a CTA: one task per CTA, its levels split over them
 constexpr int kBatchKMax = 8;   // longest chunk of a task (two levels per warp)
 
+// Input rows a task keeps in flight: at least two groups of `rows`.
+__host__ __device__ constexpr int batch_ring_depth(int rows) { return 2 * rows > kRingDepth ? 2 * rows : kRingDepth; }
+
 // Shared memory of a task pipeline of P planes with `rows` rows per barrier:
 // the input ring plus two hand-off slots per warp boundary.
-constexpr int batch_smem_words(int planes, int rows) {
-    return (kRingDepth + 2 * rows * (kBatchWarps - 1)) * planes * 32;
+__host__ __device__ constexpr int batch_smem_words(int planes, int rows) {
+    return (batch_ring_depth(rows) + 2 * rows * (kBatchWarps - 1)) * planes * 32;
 }
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
@@ -65,10 +68,11 @@ template <class R, int K, int ROWS, int SMEM>
 __device__ __forceinline__ void batch_run_task(const strip_task& t, const lane_geom<1>& geom, uint32_t* smem) {
     constexpr int L = K >= kBatchWarps ? K / kBatchWarps : 1;
     constexpr int W = K / L;
-    static_assert(pipe_rows_smem_words<R, K, 1, L, kRingDepth, ROWS>() <= SMEM,
+    constexpr int DEPTH = batch_ring_depth(ROWS);
+    static_assert(pipe_rows_smem_words<R, K, 1, L, DEPTH, ROWS>() <= SMEM,
                   "task pipeline larger than the CTA's shared memory");
     if ((int)(threadIdx.x >> 5) < W)
-        pipe_run_rows<R, K, 1, L, kRingDepth, ROWS>(t, geom, smem);
+        pipe_run_rows<R, K, 1, L, DEPTH, ROWS>(t, geom, smem);
     else
         pipe_rows_idle<K, L, ROWS>(t);
 }
