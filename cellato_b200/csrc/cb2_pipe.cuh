@@ -296,7 +296,7 @@ __device__ __forceinline__ void pipe_run_rows(const strip_task& t, const lane_ge
     // a compile-time constant and the branch folds.
     auto sweep = [&](auto parity) {
         constexpr int PAR = decltype(parity)::value;
-        const int64_t tbase = (PAR < 0 ? t.t0 : ((t.t0 & ~(int64_t)1) | PAR)) + (int64_t)warp * L;
+        [[maybe_unused]] const int64_t tbase = (PAR < 0 ? t.t0 : ((t.t0 & ~(int64_t)1) | PAR)) + (int64_t)warp * L;
         for (int st = 0; st < steps; ++st) {
             uint32_t rows[RPS][V][P];
             if (warp == 0) {
