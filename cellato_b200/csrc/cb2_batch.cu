@@ -71,14 +71,15 @@ constexpr int kBuiltinRows = 4;    // rows each warp passes on per barrier (2: 1
 // drops the eight-generation pipelines (a batch whose chunks are at most 4).
 template <int KMAX>
 struct builtin_rules {
-    static constexpr int kSmemWords = batch_smem_words(kBuiltinPlanes, kBuiltinRows);
+    static constexpr int kWarps = kBatchKindWarps[kBatchBuiltin];
+    static constexpr int kSmemWords = batch_smem_words(kBuiltinPlanes, kBuiltinRows, kWarps);
     static constexpr bool kTimed = false;  // the networks read neither time, seed nor global rows
     __device__ __forceinline__ static void run(int automaton, int k, const strip_task& t, const lane_geom<1>& geom,
                                                uint32_t* smem) {
         switch (automaton) {
-        case 0: batch_run_rule<game_of_life, KMAX, kBuiltinRows, kSmemWords>(t, k, geom, smem); break;
-        case 1: batch_run_rule<wire, KMAX, kBuiltinRows, kSmemWords>(t, k, geom, smem); break;
-        default: batch_run_rule<excitable, KMAX, kBuiltinRows, kSmemWords>(t, k, geom, smem); break;
+        case 0: batch_run_rule<game_of_life, KMAX, kBuiltinRows, kSmemWords, kWarps>(t, k, geom, smem); break;
+        case 1: batch_run_rule<wire, KMAX, kBuiltinRows, kSmemWords, kWarps>(t, k, geom, smem); break;
+        default: batch_run_rule<excitable, KMAX, kBuiltinRows, kSmemWords, kWarps>(t, k, geom, smem); break;
         }
     }
 };
@@ -140,7 +141,7 @@ int batch_engine::init(int task_capacity, int grid_capacity, int kmax_, long lon
     for (int k = 0; k < 2; ++k) {
         const void* fn = batch_kernel_for(k, kmax);
         int per_sm = 0;
-        if (fn) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBatchWarps * 32, 0);
+        if (fn) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBatchKindWarps[k] * 32, 0);
         kind_blocks[k] = std::max(1, per_sm) * std::max(1, sms);
     }
     blocks = kind_blocks[kBatchBuiltin];
@@ -309,7 +310,7 @@ int batch_engine::capture(int k) {
     cudaMemsetAsync(d_counters, 0, sizeof(unsigned) * 2, cap_stream);  // head, error
     cudaMemsetAsync(d_task_done, 0, sizeof(unsigned) * (size_t)task_cap, cap_stream);
     void* args[] = {&a};
-    cudaLaunchKernel(fn, dim3((unsigned)kind_blocks[k]), dim3(kBatchWarps * 32), args, 0, cap_stream);
+    cudaLaunchKernel(fn, dim3((unsigned)kind_blocks[k]), dim3(kBatchKindWarps[k] * 32), args, 0, cap_stream);
     const int nflip = grid_cap;
     batch_flip_kernel<<<(nflip + 255) / 256, 256, 0, cap_stream>>>(d_grids, d_odd, d_counters + 2);
     e = cudaStreamEndCapture(cap_stream, &graph[k]);

@@ -75,6 +75,12 @@ struct batch_tiling {
 // memory, so they get a kernel of their own).
 enum batch_kind { kBatchBuiltin = 0, kBatchAll = 1 };
 
+// Warps of a CTA (one task) in each kind's kernel.  Two warps per task for
+// the networks (four levels each, twice the resident CTAs) measured slower:
+// 18.1 against 19.1 Tcell/s on the batched workload, 12.4 against 15.0 served
+// at 20000 req/s -- the longer chain links cost more than the occupancy gains.
+constexpr int kBatchKindWarps[2] = {4, 4};
+
 // The kernel of kind kBatchAll (cb2_generic_batch.cu); null when the library
 // has no lowered DSL automata.
 const void* generic_batch_kernel();

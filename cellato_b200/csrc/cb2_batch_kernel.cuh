@@ -16,16 +16,15 @@
 
 namespace cb2 {
 
-constexpr int kBatchWarps = 4;  // warps of a CTA: one task per CTA, its levels split over them
-constexpr int kBatchKMax = 8;   // longest chunk of a task (two levels per warp)
+constexpr int kBatchKMax = 8;  // longest chunk of a task
 
 // Input rows a task keeps in flight: at least two groups of `rows`.
 __host__ __device__ constexpr int batch_ring_depth(int rows) { return 2 * rows > kRingDepth ? 2 * rows : kRingDepth; }
 
-// Shared memory of a task pipeline of P planes with `rows` rows per barrier:
-// the input ring plus two hand-off slots per warp boundary.
-__host__ __device__ constexpr int batch_smem_words(int planes, int rows) {
-    return (batch_ring_depth(rows) + 2 * rows * (kBatchWarps - 1)) * planes * 32;
+// Shared memory of a task pipeline of P planes with `rows` rows per barrier
+// over `warps` warps: the input ring plus two hand-off slots per warp boundary.
+__host__ __device__ constexpr int batch_smem_words(int planes, int rows, int warps) {
+    return (batch_ring_depth(rows) + 2 * rows * (warps - 1)) * planes * 32;
 }
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
@@ -59,14 +58,14 @@ __device__ __forceinline__ int64_t chunk_start(const batch_grid_desc& g, int c) 
     return t;
 }
 
-// One chunk of K generations of one task on the whole CTA: the level pipeline
-// of pipe_run_rows with the K levels split over the warps (K = 8: two levels
-// per warp, K = 4: one), which divides a task's latency -- and with it the
-// length of a grid's chain of chunks -- by the number of warps.  Chunks
-// shorter than the CTA (K = 2, 1) leave warps idle at the barriers.
-template <class R, int K, int ROWS, int SMEM>
+// One chunk of K generations of one task on the whole CTA of WARPS warps: the
+// level pipeline of pipe_run_rows with the K levels split over the warps,
+// which divides a task's latency -- and with it the length of a grid's chain
+// of chunks -- by the number of warps.  Chunks shorter than the CTA leave
+// warps idle at the barriers.
+template <class R, int K, int ROWS, int SMEM, int WARPS>
 __device__ __forceinline__ void batch_run_task(const strip_task& t, const lane_geom<1>& geom, uint32_t* smem) {
-    constexpr int L = K >= kBatchWarps ? K / kBatchWarps : 1;
+    constexpr int L = K >= WARPS ? K / WARPS : 1;
     constexpr int W = K / L;
     constexpr int DEPTH = batch_ring_depth(ROWS);
     static_assert(pipe_rows_smem_words<R, K, 1, L, DEPTH, ROWS>() <= SMEM,
@@ -78,22 +77,23 @@ __device__ __forceinline__ void batch_run_task(const strip_task& t, const lane_g
 }
 
 // One task of rule R with the chunk length k of the task (1, 2, 4, or KMAX).
-template <class R, int KMAX, int ROWS, int SMEM>
+template <class R, int KMAX, int ROWS, int SMEM, int WARPS>
 __device__ __forceinline__ void batch_run_rule(const strip_task& t, int k, const lane_geom<1>& geom, uint32_t* smem) {
     switch (k) {
-    case 1: batch_run_task<R, 1, ROWS, SMEM>(t, geom, smem); break;
-    case 2: batch_run_task<R, 2, ROWS, SMEM>(t, geom, smem); break;
-    case 4: batch_run_task<R, 4, ROWS, SMEM>(t, geom, smem); break;
+    case 1: batch_run_task<R, 1, ROWS, SMEM, WARPS>(t, geom, smem); break;
+    case 2: batch_run_task<R, 2, ROWS, SMEM, WARPS>(t, geom, smem); break;
+    case 4: batch_run_task<R, 4, ROWS, SMEM, WARPS>(t, geom, smem); break;
     default:
-        if constexpr (KMAX >= 8) batch_run_task<R, 8, ROWS, SMEM>(t, geom, smem);
+        if constexpr (KMAX >= 8) batch_run_task<R, 8, ROWS, SMEM, WARPS>(t, geom, smem);
         break;
     }
 }
 
-// The persistent kernel.  D is the rule set: D::kSmemWords shared words per
-// CTA and D::run(automaton, k, task, geom, smem) running one task.
+// The persistent kernel.  D is the rule set: D::kWarps warps and D::kSmemWords
+// shared words per CTA, and D::run(automaton, k, task, geom, smem) running one
+// task.
 template <class D>
-__global__ void __launch_bounds__(kBatchWarps * 32) batch_kernel(batch_args a) {
+__global__ void __launch_bounds__(D::kWarps * 32) batch_kernel(batch_args a) {
     __shared__ __align__(16) uint32_t smem[D::kSmemWords];
     __shared__ unsigned s_task;
     __shared__ int s_ok;

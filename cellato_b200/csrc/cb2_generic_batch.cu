@@ -24,8 +24,9 @@ namespace {
 
 constexpr int kNetRows = 4;  // the hand-written networks, as in their own batch kernel
 constexpr int kDslRows = 2;
-constexpr int kSmem = batch_smem_words(kMaxPlanes, kDslRows);
-static_assert(batch_smem_words(3, kNetRows) <= kSmem, "network pipelines larger than the lowered rules'");
+constexpr int kWarps = kBatchKindWarps[kBatchAll];
+constexpr int kSmem = batch_smem_words(kMaxPlanes, kDslRows, kWarps);
+static_assert(batch_smem_words(3, kNetRows, kWarps) <= kSmem, "network pipelines larger than the lowered rules'");
 
 template <class... C>
 struct config_list {};
@@ -37,7 +38,7 @@ __device__ __forceinline__ void run_lowered(int id, int k, const strip_task& t, 
                                             uint32_t* smem) {
     if constexpr (!std::is_same_v<C, list_end>) {
         if (id == I)
-            batch_run_rule<ast_rule<C>, kBatchKMax, kDslRows, kSmem>(t, k, geom, smem);
+            batch_run_rule<ast_rule<C>, kBatchKMax, kDslRows, kSmem, kWarps>(t, k, geom, smem);
         else
             run_lowered<I + 1, Rest...>(id, k, t, geom, smem);
     }
@@ -64,14 +65,15 @@ using all_configs = config_list<CB2_DSL_CONFIGS(CB2_CONFIG_TYPE) list_end>;
 #undef CB2_USER_TYPE
 
 struct all_rules {
+    static constexpr int kWarps = cb2::kWarps;
     static constexpr int kSmemWords = kSmem;
     static constexpr bool kTimed = true;
     __device__ __forceinline__ static void run(int automaton, int k, const strip_task& t, const lane_geom<1>& geom,
                                                uint32_t* smem) {
         switch (automaton) {
-        case 0: batch_run_rule<game_of_life, kBatchKMax, kNetRows, kSmem>(t, k, geom, smem); break;
-        case 1: batch_run_rule<wire, kBatchKMax, kNetRows, kSmem>(t, k, geom, smem); break;
-        case 2: batch_run_rule<excitable, kBatchKMax, kNetRows, kSmem>(t, k, geom, smem); break;
+        case 0: batch_run_rule<game_of_life, kBatchKMax, kNetRows, kSmem, kWarps>(t, k, geom, smem); break;
+        case 1: batch_run_rule<wire, kBatchKMax, kNetRows, kSmem, kWarps>(t, k, geom, smem); break;
+        case 2: batch_run_rule<excitable, kBatchKMax, kNetRows, kSmem, kWarps>(t, k, geom, smem); break;
         default: lowered<all_configs>::run(automaton, k, t, geom, smem); break;
         }
     }
