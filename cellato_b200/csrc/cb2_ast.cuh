@@ -284,7 +284,8 @@ __device__ __forceinline__ uint32_t bernoulli_word(const cell_ctx& c, uint64_t l
             // as independent instructions and compared with digits known at compile
             // time; draws past the one that resolves the last lane are not used.
             // A warp of 1024 cells needs about 11 digits, so a pair, whose shuffles
-            // make the tail dearer, computes 12 up front.
+            // make the tail dearer, computes 12 up front (8: lightning-forest 0.99
+            // against 1.15 Tcell/s).
             uint32_t active = 0xffffffffu, result = 0;
             auto digit = [&](uint64_t& rem, uint32_t bits) {
                 if (rem >= d - rem) {
