@@ -266,6 +266,59 @@ void orc_checksum(const uint8_t* cells, int64_t X, int64_t Y, const int64_t* val
     }
 }
 
+/* The same checksum computed from bit planes (32-bit words, P planes of Y   */
+/* rows of X/32 words), for grids too large to hold one byte per cell: each  */
+/* word adds popcount(minterm(state) & tile columns) * value for each state. */
+/* X must be a multiple of 32.                                               */
+void orc_checksum_planes(const orc_word* planes, int64_t X, int64_t Y, int P, const int64_t* values,
+                         uint64_t out[16]) {
+    int64_t tw = (X + 3) / 4, th = (Y + 3) / 4, XW = X / 32, plane = XW * Y;
+    memset(out, 0, 16 * sizeof(uint64_t));
+    for (int64_t y = 0; y < Y; ++y) {
+        int ty = (int)(y / th);
+        for (int64_t xw = 0; xw < XW; ++xw) {
+            orc_word v[8];
+            for (int b = 0; b < P; ++b) v[b] = planes[b * plane + y * XW + xw];
+            for (int tx = 0; tx < 4; ++tx) {
+                int64_t x0 = tx * tw, x1 = x0 + tw < X ? x0 + tw : X;
+                int64_t lo = x0 > xw * 32 ? x0 - xw * 32 : 0, hi = x1 < xw * 32 + 32 ? x1 - xw * 32 : 32;
+                if (lo >= hi) continue;
+                orc_word cols = (hi - lo == 32) ? ~(orc_word)0 : ((((orc_word)1 << (hi - lo)) - 1) << lo);
+                for (int s = 0; s < (1 << P); ++s) {
+                    uint64_t n = (uint64_t)__builtin_popcount(eq_state(v, P, s) & cols);
+                    out[ty * 4 + tx] += n * (uint64_t)values[s];
+                }
+            }
+        }
+    }
+}
+
+/* orc_init_cells written straight into bit planes (same cell stream: cell   */
+/* y*X + x draws index y*X + x), for grids too large for a byte per cell;    */
+/* rows [row_first, row_first + row_count) only, so threads can share it.   */
+int orc_init_bit_planes_rows(orc_word* planes, int64_t X, int64_t Y, int P, uint64_t seed, const uint64_t* thr,
+                             int nthr, int64_t row_first, int64_t row_count) {
+    if (X % 32 || P < 1 || P > 8 || row_first < 0 || row_count < 0 || row_first + row_count > Y) return -1;
+    int64_t XW = X / 32, plane = XW * Y;
+    for (int64_t y = row_first; y < row_first + row_count; ++y)
+        for (int64_t xw = 0; xw < XW; ++xw) {
+            orc_word w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            for (int i = 0; i < 32; ++i) {
+                uint64_t u = orc_splitmix64(seed, (uint64_t)(y * X + xw * 32 + i)) >> 11;
+                int s = 0;
+                while (s < nthr && u >= thr[s]) ++s;
+                for (int b = 0; b < P; ++b) w[b] |= (orc_word)((s >> b) & 1) << i;
+            }
+            for (int b = 0; b < P; ++b) planes[b * plane + y * XW + xw] = w[b];
+        }
+    return 0;
+}
+
+int orc_init_bit_planes(orc_word* planes, int64_t X, int64_t Y, int P, uint64_t seed, const uint64_t* thr,
+                        int nthr) {
+    return orc_init_bit_planes_rows(planes, X, Y, P, seed, thr, nthr, 0, Y);
+}
+
 /* ------------------------------------------------------------------------ */
 /* Layout packing (host byte images of the reference's grids).               */
 /* ------------------------------------------------------------------------ */

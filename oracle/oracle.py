@@ -56,6 +56,10 @@ def _lib():
         lib.orc_step_bit_planes.argtypes = [ctypes.c_int, _i64, _i64, _u32p, _u32p]
         lib.orc_run_bit_planes.argtypes = [ctypes.c_int, _i64, _i64, _i64, _u32p]
         lib.orc_checksum.argtypes = [_u8p, _i64, _i64, _i64p, _u64p]
+        lib.orc_checksum_planes.argtypes = [_u32p, _i64, _i64, ctypes.c_int, _i64p, _u64p]
+        lib.orc_init_bit_planes.argtypes = [_u32p, _i64, _i64, ctypes.c_int, ctypes.c_uint64, _u64p, ctypes.c_int]
+        lib.orc_init_bit_planes_rows.argtypes = [_u32p, _i64, _i64, ctypes.c_int, ctypes.c_uint64, _u64p,
+                                                 ctypes.c_int, _i64, _i64]
         for name in ("orc_pack_bit_planes", "orc_unpack_bit_planes"):
             getattr(lib, name).argtypes = [_u8p, _i64, _i64, ctypes.c_int, _u8p]
         for name in ("orc_pack_bit_array", "orc_unpack_bit_array", "orc_pack_tiled", "orc_unpack_tiled"):
@@ -95,6 +99,10 @@ def _reflib():
         lib.ref_bench.restype = ctypes.c_double
         lib.ref_run_seeded.argtypes = [ctypes.c_int] * 7 + [_u8p, _u8p, ctypes.c_char_p, ctypes.c_int]
         lib.ref_automaton_id.argtypes = [ctypes.c_char_p]
+        lib.ref_bench_planes64.argtypes = [ctypes.c_int] * 5 + [_u64p]
+        lib.ref_bench_planes64.restype = ctypes.c_double
+        lib.ref_run_planes64.argtypes = [ctypes.c_int] * 5 + [_u64p, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                                              ctypes.POINTER(_u64p), ctypes.c_int]
         _ref = lib
     return _ref
 
@@ -157,6 +165,39 @@ def checksum(cells: np.ndarray, values=None) -> list[int]:
 
 def checksum_str(cells: np.ndarray, values=None) -> str:
     return "-".join(str(v) for v in checksum(cells, values))
+
+
+def init_bit_planes(x: int, y: int, planes: int, seed: int, thr: np.ndarray, threads: int = 1) -> np.ndarray:
+    """init_cells written straight into bit planes: uint32 array (planes, y, x/32),
+    generated by `threads` host threads over row ranges."""
+    out = np.empty((planes, y, x // 32), dtype=np.uint32)
+    thr = np.ascontiguousarray(thr, dtype=np.uint64)
+    lib = _lib()
+    threads = max(1, min(threads, y))
+    bounds = [y * t // threads for t in range(threads + 1)]
+
+    def rows(t):
+        return lib.orc_init_bit_planes_rows(_p(out, _u32p), x, y, planes, seed, _p(thr, _u64p), len(thr),
+                                            bounds[t], bounds[t + 1] - bounds[t])
+    if threads == 1:
+        rcs = [rows(0)]
+    else:
+        from concurrent.futures import ThreadPoolExecutor  # ctypes releases the GIL during the calls
+        with ThreadPoolExecutor(threads) as pool:
+            rcs = list(pool.map(rows, range(threads)))
+    if any(rcs):
+        raise ValueError(f"orc_init_bit_planes_rows failed ({rcs})")
+    return out
+
+
+def checksum_planes(planes: np.ndarray, x: int, y: int, n_planes: int, values=None) -> list[int]:
+    """The 16-tile checksum computed from bit planes (any word size: the bytes are the same)."""
+    w = np.ascontiguousarray(planes).view(np.uint32)
+    assert w.size == n_planes * y * x // 32
+    vals = np.arange(256, dtype=np.int64) if values is None else np.ascontiguousarray(values, dtype=np.int64)
+    out = np.zeros(16, dtype=np.uint64)
+    _lib().orc_checksum_planes(_p(w, _u32p), x, y, n_planes, _p(vals, _i64p), _p(out, _u64p))
+    return [int(v) for v in out]
 
 
 def pack(layout: str, cells: np.ndarray, planes: int, word_bits: int) -> np.ndarray:
@@ -242,6 +283,37 @@ def ref_pack(automaton: int, layout: str, cells: np.ndarray, word_bits: int) -> 
     if n < 0:
         raise ValueError(f"ref_pack failed ({n})")
     return out[:n].copy()
+
+
+def ref_run_planes64(automaton: int, planes: np.ndarray, x: int, y: int, steps: int, checkpoints=(), seed: int = 42,
+                     report_every: int = 0):
+    """Reference CPU simple traverser, bit_planes layout, 64-bit words, over
+    caller-given planes (uint64 (P, y, x/64), or any array of those bytes).
+    Returns (final planes, {checkpoint: planes after that generation})."""
+    p = np.ascontiguousarray(planes).view(np.uint64).copy()
+    cps = [int(c) for c in checkpoints if 0 < int(c) < steps]
+    snaps = [np.empty_like(p) for _ in cps]
+    cp_arr = (ctypes.c_int * max(1, len(cps)))(*cps)
+    snap_ptrs = (_u64p * max(1, len(cps)))(*[_p(s_, _u64p) for s_ in snaps])
+    rc = _reflib().ref_run_planes64(automaton, x, y, steps, seed, _p(p, _u64p), cp_arr, len(cps), snap_ptrs,
+                                    report_every)
+    if rc:
+        raise ValueError(f"ref_run_planes64 failed ({rc})")
+    out = dict(zip(cps, snaps))
+    if steps in [int(c) for c in checkpoints]:
+        out[steps] = p
+    return p, out
+
+
+def ref_bench_planes64(automaton: int, planes: np.ndarray, x: int, y: int, steps: int, threads: int) -> float:
+    """Seconds taken by the slowest of `threads` host threads, each running the
+    reference CPU traverser (bit_planes, 64-bit words) on its band of y/threads
+    rows of the grid held in `planes` (any array of the plane bytes)."""
+    p = np.ascontiguousarray(planes).view(np.uint64)
+    s = _reflib().ref_bench_planes64(automaton, x, y, steps, threads, _p(p, _u64p))
+    if s < 0:
+        raise RuntimeError(f"ref_bench_planes64 failed ({s})")
+    return float(s)
 
 
 def ref_bench(automaton: int, cells: np.ndarray, steps: int, threads: int, layout: str = "bit_planes",

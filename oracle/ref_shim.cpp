@@ -16,9 +16,11 @@
 #include <atomic>
 #include <chrono>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "cellato/experiments/run_params.hpp"
@@ -206,6 +208,129 @@ int ref_pack(int automaton, int layout, int word_bits, int x, int y, const uint8
     } catch (...) {
         return -10;
     }
+}
+
+// Full-size runs: the reference CPU simple traverser with the bit_planes
+// layout and 64-bit words over planes the caller provides (P planes of y rows
+// of x/64 words, plane-major), skipping the standard grid, which at 65536^2
+// would take 16 GiB of enum cells.  The grid is built with the reference's
+// own sized constructor (memory/bit_planes_grid.hpp:71-78) and filled through
+// data() (:202-212).  `planes` is overwritten with the result.  After
+// generation checkpoints[i] (1 <= c <= steps) the planes are copied to
+// snapshots[i] (same size as `planes`) from the traverser's per-step callback
+// (traversers/cpu/simple.hpp:59-84).  Progress goes to stderr every
+// `report_every` generations (0: never).  Returns 0, or a negative code.
+int ref_run_planes64(int automaton, int x, int y, int steps, int seed, uint64_t* planes, const int* checkpoints,
+                     int n_checkpoints, uint64_t* const* snapshots, int report_every) {
+    try {
+        return with_automaton(automaton, L_BIT_PLANES, 64, [&]<typename suite>() {
+            using automaton_t = typename suite::automaton;
+            if constexpr (!std::is_same_v<suite, ts::on_cpu::using_<std::uint64_t>::bit_planes<automaton_t>>) {
+                return -3; // only the 64-bit bit_planes suite is requested (with_automaton is a runtime switch)
+            } else {
+            using grid_t = typename suite::grid_t;
+            using traverser_t = typename suite::traverser_t;
+            constexpr int P = grid_t::needed_bits;
+            const std::size_t words = (std::size_t)y * (std::size_t)(x / 64);
+            if (x % 64 || x <= 0 || y <= 0 || steps < 0) return -4;
+            grid_t grid((std::size_t)y, (std::size_t)x);
+            auto dst = grid.data();
+            for (int p = 0; p < P; ++p) std::memcpy(dst[p], planes + p * words, words * sizeof(uint64_t));
+
+            cellato::run::run_params params;
+            params.x_size = x;
+            params.y_size = y;
+            params.steps = steps;
+            params.seed = seed;
+            traverser_t traverser;
+            traverser.init(std::move(grid), params);
+            auto t0 = std::chrono::steady_clock::now();
+            traverser.run(steps, [&](int step, grid_t& g) {
+                if (step <= 0) return;
+                for (int i = 0; i < n_checkpoints; ++i)
+                    if (checkpoints[i] == step) {
+                        auto src = g.data();
+                        for (int p = 0; p < P; ++p)
+                            std::memcpy(snapshots[i] + p * words, src[p], words * sizeof(uint64_t));
+                    }
+                if (report_every > 0 && step % report_every == 0) {
+                    double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+                    std::fprintf(stderr, "ref_run_planes64: automaton %d generation %d/%d, %.1f s\n", automaton,
+                                 step, steps, s);
+                }
+            });
+            grid_t result = traverser.fetch_result();
+            auto src = result.data();
+            for (int p = 0; p < P; ++p) std::memcpy(planes + p * words, src[p], words * sizeof(uint64_t));
+            return 0;
+            }
+        });
+    } catch (...) {
+        return -10;
+    }
+}
+
+// Throughput sample of the reference CPU traverser (bit_planes layout, 64-bit
+// words) on a grid given as planes (P planes of y rows of x/64 words): the
+// rows are split into `threads` bands of y/threads rows, and each host thread
+// runs the reference traverser on its band as a grid of its own (a torus of
+// the band's rows), so the threads together advance every cell of the grid
+// once per generation; threads = 1 runs the whole grid.  Returns the wall
+// time in seconds of the slowest thread for `steps` generations (init and
+// fetch outside the timed region), or a negative value on error.
+double ref_bench_planes64(int automaton, int x, int y, int steps, int threads, const uint64_t* planes) {
+    if (threads < 1 || x % 64 || x <= 0 || y % threads || steps < 0) return -2.0;
+    const int rows = y / threads;
+    std::vector<double> secs((std::size_t)threads, -1.0);
+    std::atomic<int> ready{0};
+    auto body = [&](int t) {
+        int rc = -1;
+        try {
+            rc = with_automaton(automaton, L_BIT_PLANES, 64, [&]<typename suite>() {
+                using automaton_t = typename suite::automaton;
+                if constexpr (!std::is_same_v<suite, ts::on_cpu::using_<std::uint64_t>::bit_planes<automaton_t>>) {
+                    return -3;
+                } else {
+                    using grid_t = typename suite::grid_t;
+                    using traverser_t = typename suite::traverser_t;
+                    constexpr int P = grid_t::needed_bits;
+                    const std::size_t words = (std::size_t)y * (std::size_t)(x / 64);
+                    const std::size_t band_words = (std::size_t)rows * (std::size_t)(x / 64);
+                    grid_t grid((std::size_t)rows, (std::size_t)x);
+                    auto dst = grid.data();
+                    for (int p = 0; p < P; ++p)
+                        std::memcpy(dst[p], planes + p * words + (std::size_t)t * band_words,
+                                    band_words * sizeof(uint64_t));
+                    cellato::run::run_params params;
+                    params.x_size = x;
+                    params.y_size = rows;
+                    params.steps = steps;
+                    traverser_t traverser;
+                    traverser.init(std::move(grid), params);
+                    ready.fetch_add(1);
+                    while (ready.load() < threads) std::this_thread::yield();
+                    auto t0 = std::chrono::steady_clock::now();
+                    traverser.run(steps);
+                    auto t1 = std::chrono::steady_clock::now();
+                    secs[(std::size_t)t] = std::chrono::duration<double>(t1 - t0).count();
+                    grid_t result = traverser.fetch_result();
+                    (void)result;
+                    return 0;
+                }
+            });
+        } catch (...) {
+        }
+        if (rc != 0 && secs[(std::size_t)t] < 0) ready.fetch_add(1);  // release the others
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t) pool.emplace_back(body, t);
+    for (auto& th : pool) th.join();
+    double worst = 0;
+    for (double s : secs) {
+        if (s < 0) return -1.0;
+        worst = s > worst ? s : worst;
+    }
+    return worst;
 }
 
 // Throughput sample for the CPU baseline: `threads` host threads each run an
