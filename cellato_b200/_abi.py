@@ -99,6 +99,8 @@ _vpp = ctypes.POINTER(ctypes.c_void_p)
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _i64p = ctypes.POINTER(ctypes.c_int64)
 _tp = ctypes.POINTER(Tuning)
+# cb2_halo_exchange_fn: (user, buffer, k, stream) -> status
+HALO_EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p)
 
 # name -> (restype, argtypes)
 _SIGNATURES = {
@@ -108,15 +110,20 @@ _SIGNATURES = {
     "cb2_automaton_info": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
                                           ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "cb2_automaton_count": (ctypes.c_int, []),
+    "cb2_automaton_fingerprint": (ctypes.c_int, [ctypes.c_int, _u64p]),
     "cb2_automaton_values": (ctypes.c_int, [ctypes.c_int, _i64p, ctypes.c_int]),
     "cb2_run_bit_planes": (ctypes.c_int, [ctypes.c_int, _vpp, _vpp, _i64, _i64, _i64, _tp, _vp,
                                           ctypes.POINTER(ctypes.c_int)]),
     "cb2_run_bit_planes_at": (ctypes.c_int, [ctypes.c_int, _vpp, _vpp, _i64, _i64, _i64, _i64, ctypes.c_uint64, _tp,
                                              _vp, ctypes.POINTER(ctypes.c_int)]),
-    "cb2_run_bit_planes_in_place": (ctypes.c_int, [ctypes.c_int, _vpp, _i64, _i64, _i64, _tp, _vp]),
+    "cb2_run_bit_planes_in_place": (ctypes.c_int, [ctypes.c_int, _vpp, _i64, _i64, _i64, _i64, ctypes.c_uint64, _tp,
+                                                    _vp]),
     "cb2_band_pass": (ctypes.c_int, [ctypes.c_int, _vpp, _vpp, _i64, _i64, _i64, _i64, ctypes.c_int, _tp, _vp]),
     "cb2_band_pass_at": (ctypes.c_int, [ctypes.c_int, _vpp, _vpp, _i64, _i64, _i64, _i64, ctypes.c_int, _i64,
                                         ctypes.c_uint64, _i64, _i64, _tp, _vp]),
+    "cb2_band_schedule": (_i64, [_i64, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _i64]),
+    "cb2_band_run": (ctypes.c_int, [ctypes.c_int, _vpp, _vpp, _i64, _i64, ctypes.c_int, _i64, _i64, ctypes.c_uint64,
+                                    _i64, _i64, _tp, HALO_EXCHANGE_FN, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_int)]),
     "cb2_fill_random_planes": (ctypes.c_int, [ctypes.c_int, _vpp, _i64, _i64, _i64, _i64, ctypes.c_uint64, _u64p,
                                               ctypes.c_int, _vp]),
     "cb2_checksum_planes": (ctypes.c_int, [ctypes.c_int, _vpp, _i64, _i64, _i64, _i64, _i64, _i64, _i64p,

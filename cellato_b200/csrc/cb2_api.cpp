@@ -263,6 +263,18 @@ int cb2_automaton_info(int id, const char** name, int* planes, int* states) {
 
 int cb2_automaton_count(void) { return automaton_count(); }
 
+int cb2_automaton_fingerprint(int id, uint64_t* fingerprint) {
+    const automaton_desc* d = automaton_at(id);
+    if (!d) return fail(CB2_ENOTFOUND, "unknown automaton id " + std::to_string(id));
+    if (!fingerprint) return fail(CB2_EINVAL, "null output");
+    const uint64_t fp = id < kNumBuiltin ? builtin_fingerprint(id) : d->fingerprint;
+    if (!fp)
+        return fail(CB2_ENOTFOUND, "the library was built without the Cellato headers and cannot tell which rule "
+                                   "automaton '" + std::string(d->name) + "' is");
+    *fingerprint = fp;
+    return CB2_OK;
+}
+
 int cb2_automaton_values(int id, int64_t* values, int capacity) {
     const automaton_desc* d = automaton_at(id);
     if (!d) return fail(CB2_ENOTFOUND, "unknown automaton id " + std::to_string(id));
@@ -661,9 +673,10 @@ int cb2_measure_lop3_peak(double* ops_per_second) {
 
 int cb2_network_ops(int automaton, double* alu, double* shuffles) {
     // Per 32-bit word per generation (cb2_rules.cuh): two funnel shifts for
-    // the west/east neighbour words, plus the rule's logic ops; two shuffles
-    // per lane per row, shared by the lane's V = 2 words.
-    static const double kLogic[kNumBuiltin] = {10, 11, 7};
+    // the west/east neighbour words, plus the rule's logic ops (game of life
+    // 10, wireworld 10, greenberg-hastings 7 three-input operations); two
+    // shuffles per lane per row, shared by the lane's V = 2 words.
+    static const double kLogic[kNumBuiltin] = {10, 10, 7};
     if (automaton >= kNumBuiltin && automaton < automaton_count())
         return fail(CB2_EINVAL, "no static operation count for a lowered DSL automaton");
     if (automaton < 0 || automaton >= kNumBuiltin) return fail(CB2_ENOTFOUND, "unknown automaton");

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "cb2_internal.h"
 
@@ -93,6 +94,103 @@ int cb2_band_pass_at(int automaton, void* const* in, void* const* out, int64_t x
     cudaError_t e = launch_strip_window(g, (const uint32_t*)in[0], (uint32_t*)out[0], plan, (int)row_first,
                                         (int)rows_out, (cudaStream_t)stream, time_step, seed, row0, global_rows);
     if (e != cudaSuccess) return cuda_err(e, "band pass launch");
+    return CB2_OK;
+}
+
+int64_t cb2_band_schedule(int64_t steps, int temporal_steps, int ghost, int* depths, int64_t capacity) {
+    if (steps < 0 || temporal_steps < 1 || ghost < 1 || capacity < 0 || (capacity && !depths)) {
+        set_error("band schedule needs steps >= 0, temporal_steps >= 1, ghost >= 1 and room for the depths");
+        return CB2_EINVAL;
+    }
+    const int k_main = temporal_steps < ghost ? temporal_steps : ghost;
+    int64_t n = 0, left = steps;
+    while (left > 0) {
+        int k = k_main;
+        while (k > left) k /= 2;  // the remainder's binary digits, largest first
+        if (n < capacity) depths[n] = k;
+        ++n;
+        left -= k;
+    }
+    return n;
+}
+
+int cb2_band_run(int automaton, void* const* a, void* const* b, int64_t x_size, int64_t band_rows, int ghost,
+                 int64_t time_step, int64_t steps, uint64_t seed, int64_t global_row0, int64_t global_rows,
+                 const cb2_tuning* tuning, cb2_halo_exchange_fn exchange, void* user, void* stream,
+                 void* exchange_stream, int* result_in_b) {
+    if (!exchange || band_rows < 1 || ghost < 1 || steps < 0 || time_step < 0) {
+        set_error("band run needs an exchange function, band rows, ghost rows, steps >= 0 and time_step >= 0");
+        return CB2_EINVAL;
+    }
+    const int64_t rows_total = band_rows + 2 * (int64_t)ghost;
+    grid_geom g;
+    int rc = make_geom(automaton, x_size, rows_total, &g);
+    if (rc) return rc;
+    if ((rc = check_planes(g, a, "a")) || (rc = check_planes(g, b, "b"))) return rc;
+    int k_main = tuning && tuning->temporal_steps ? tuning->temporal_steps : 0;
+    if (!k_main) {  // the single-grid plan of a grid of the band's size
+        grid_geom band = g;
+        band.h = (int32_t)band_rows;
+        band.y_size = band_rows;
+        band.plane_words = (int64_t)g.wd * band_rows;
+        cb2_tuning t0{0, 0, 0, 0, 0};
+        run_plan p;
+        if ((rc = resolve_plan(band, &t0, &p))) return rc;
+        k_main = p.k;
+    }
+    const int64_t n = cb2_band_schedule(steps, k_main, ghost, nullptr, 0);
+    if (n < 0) return (int)n;
+    std::vector<int> depths((size_t)n);
+    cb2_band_schedule(steps, k_main, ghost, depths.data(), n);
+
+    cudaStream_t s = (cudaStream_t)stream, xs = (cudaStream_t)exchange_stream;
+    cudaEvent_t ready = nullptr, landed = nullptr;
+    cudaError_t e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&landed, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        if (ready) cudaEventDestroy(ready);
+        return cuda_err(e, "band run events");
+    }
+    void* const* bufs[2] = {a, b};
+    int cur = 0;
+    int64_t t = time_step;
+    const int64_t planes_row0 = global_row0 - ghost;  // global row of the planes' row 0
+    for (int k : depths) {
+        // The exchange may only overwrite ghost rows once the previous pass,
+        // which read them, is done; it reads band rows that pass wrote.
+        if ((e = cudaEventRecord(ready, s)) != cudaSuccess || (e = cudaStreamWaitEvent(xs, ready, 0)) != cudaSuccess)
+            break;
+        if ((rc = exchange(user, cur, k, exchange_stream)) != 0) {
+            set_error("halo exchange callback failed with " + std::to_string(rc));
+            rc = CB2_EINVAL;
+            break;
+        }
+        const bool split = band_rows >= 3 * (int64_t)k;
+        if (split && (rc = cb2_band_pass_at(automaton, bufs[cur], bufs[1 - cur], x_size, rows_total, ghost + k,
+                                            band_rows - 2 * k, k, t, seed, planes_row0, global_rows, tuning,
+                                            stream)))
+            break;
+        if ((e = cudaEventRecord(landed, xs)) != cudaSuccess || (e = cudaStreamWaitEvent(s, landed, 0)) != cudaSuccess)
+            break;
+        if (split) {
+            if ((rc = cb2_band_pass_at(automaton, bufs[cur], bufs[1 - cur], x_size, rows_total, ghost, k, k, t, seed,
+                                       planes_row0, global_rows, tuning, stream)) ||
+                (rc = cb2_band_pass_at(automaton, bufs[cur], bufs[1 - cur], x_size, rows_total,
+                                       ghost + band_rows - k, k, k, t, seed, planes_row0, global_rows, tuning,
+                                       stream)))
+                break;
+        } else if ((rc = cb2_band_pass_at(automaton, bufs[cur], bufs[1 - cur], x_size, rows_total, ghost, band_rows,
+                                          k, t, seed, planes_row0, global_rows, tuning, stream))) {
+            break;
+        }
+        cur ^= 1;
+        t += k;
+    }
+    cudaEventDestroy(ready);
+    cudaEventDestroy(landed);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_err(e, "band run stream ordering");
+    if (result_in_b) *result_in_b = cur;
     return CB2_OK;
 }
 

@@ -25,6 +25,7 @@
 
 #include "cb2_ast.cuh"
 #include "cb2_dsl_configs.h"
+#include "cellato_b200/fingerprint.hpp"
 #include "cb2_internal.h"
 #include "cb2_launch.cuh"
 
@@ -58,7 +59,8 @@ struct dsl_entry {
         return v;
     }
     static automaton_desc desc(const char* name) {
-        return automaton_desc{name, dict::needed_bits, dict::number_of_values, values()};
+        constexpr uint64_t fp = ::cellato_b200::fingerprint::of<Config>();
+        return automaton_desc{name, dict::needed_bits, dict::number_of_values, values(), fp};
     }
 };
 
@@ -91,6 +93,16 @@ const dsl_table& table() {
 }
 
 } // namespace
+
+uint64_t builtin_fingerprint(int id) {
+    // the reference's own configs of the three automata the hand-written networks compute
+    switch (id) {
+    case 0: return ::cellato_b200::fingerprint::of<::game_of_life::config>();
+    case 1: return ::cellato_b200::fingerprint::of<::wire::config>();
+    case 2: return ::cellato_b200::fingerprint::of<::excitable::config>();
+    default: return 0;
+    }
+}
 
 int generic_count() { return (int)table().descs.size(); }
 

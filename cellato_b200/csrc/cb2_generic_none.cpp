@@ -10,6 +10,8 @@ namespace cb2 {
 
 int generic_count() { return 0; }
 
+uint64_t builtin_fingerprint(int) { return 0; }
+
 const automaton_desc* generic_desc(int) { return nullptr; }
 
 const std::vector<strip_variant>& generic_variants(int) {

@@ -51,6 +51,7 @@ struct automaton_desc {
     int planes;
     int states;
     const int64_t* values;  // dictionary index -> state value (the checksum sums values)
+    uint64_t fingerprint = 0;  // of the Cellato config's rule and dictionary (0: unknown)
 };
 int automaton_count();
 const automaton_desc* automaton_at(int id);  // nullptr for an unknown id
@@ -61,6 +62,10 @@ int find_automaton(const char* name);
 // kernels, indexed from 0 (= automaton id kNumBuiltin).
 int generic_count();
 const automaton_desc* generic_desc(int i);
+// Fingerprint (include/cellato_b200/fingerprint.hpp) of the Cellato config a
+// hand-written network (id < kNumBuiltin) computes, 0 when the library was
+// built without the Cellato headers.
+uint64_t builtin_fingerprint(int id);
 
 // Launches one K-generation strip pass over a whole grid (in -> out); the
 // input is generation t0 (read by time-dependent rules), seed the run's

@@ -62,12 +62,13 @@ int scratch_address(void** out) {
 } // namespace
 
 extern "C" int cb2_run_bit_planes_in_place(int automaton, void* const* planes, int64_t x_size, int64_t y_size,
-                                           int64_t steps, const cb2_tuning* tuning, void* stream) {
+                                           int64_t time_step, int64_t steps, uint64_t seed, const cb2_tuning* tuning,
+                                           void* stream) {
     cb2::grid_geom g;
     int rc = cb2::make_geom(automaton, x_size, y_size, &g);
     if (rc) return rc;
-    if (!planes || steps < 0) {
-        cb2::set_error("null plane array or negative steps");
+    if (!planes || steps < 0 || time_step < 0) {
+        cb2::set_error("null plane array, negative steps or negative time_step");
         return CB2_EINVAL;
     }
     const size_t bytes = (size_t)g.planes * (size_t)g.plane_words * 4;
@@ -87,7 +88,7 @@ extern "C" int cb2_run_bit_planes_in_place(int automaton, void* const* planes, i
     if (rc) return rc;
     uint32_t* const bufs[2] = {(uint32_t*)planes[0], (uint32_t*)scratch};
     int res = 0;
-    rc = cb2::run_chunks(g, bufs, 0, steps, tuning, (cudaStream_t)stream, &res);
+    rc = cb2::run_chunks(g, bufs, 0, steps, tuning, (cudaStream_t)stream, &res, time_step, seed);
     if (rc) return rc;
     if (res == 1) {  // an odd number of passes left the result in the scratch
         cudaError_t e = cudaMemcpyAsync(planes[0], scratch, bytes, cudaMemcpyDeviceToDevice, (cudaStream_t)stream);

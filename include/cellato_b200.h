@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define CB2_ABI_VERSION 3
+#define CB2_ABI_VERSION 4
 
 /* ---- status codes ------------------------------------------------------- */
 #define CB2_OK 0
@@ -74,6 +74,16 @@ int cb2_automaton_info(int id, const char** name, int* planes, int* states);
  * "<name>:dsl" twins of the first three) whose type-level AST
  * (core/ast.hpp) the library lowered to word-wide code at build time. */
 int cb2_automaton_count(void);
+/* Fingerprint of the rule registered as automaton `id`: a structural hash of
+ * its Cellato config's algorithm type and state dictionary
+ * (include/cellato_b200/fingerprint.hpp).  The reference instantiates each
+ * suite for the config type and so always evaluates that config's own rule
+ * (experiments/test_suites.hpp:189-195); the drop-in traverser compares this
+ * value with its config's fingerprint so that a config whose name matches a
+ * registered automaton but whose rule differs is rejected instead of run.
+ * CB2_ENOTFOUND if the id is unknown or the library was built without the
+ * Cellato headers. */
+int cb2_automaton_fingerprint(int id, uint64_t* fingerprint);
 /* State value of each dictionary index of automaton `id` (index_to_state,
  * memory/state_dictionary.hpp:10-62, as an integer): writes up to `capacity`
  * values and returns the number of states. */
@@ -120,8 +130,13 @@ int cb2_run_bit_planes_at(int automaton, void* const* a, void* const* b, int64_t
  * cudaMalloc (a host application that owns all device memory and forbids
  * plugins to allocate, or a step loop that must not allocate).  It has no
  * counterpart in the reference.  `planes` (P consecutive planes in one
- * allocation, CB2_LAYOUT_BIT_PLANES) hold the input and, in stream order,
- * receive generation `steps`.  The second buffer of the double buffer is a
+ * allocation, CB2_LAYOUT_BIT_PLANES) hold generation `time_step` and, in
+ * stream order, receive generation time_step + steps.  `time_step` and `seed`
+ * mean what they mean in cb2_run_bit_planes_at: rules that read the
+ * generation or the seed (alternate_algorithms, Margolus blocks, probability
+ * draws) need them, so a step loop of N calls passes its running generation
+ * count and one seed, and then matches one run of N*steps generations.
+ * The second buffer of the double buffer is a
  * file-scope __device__ array of CB2_STATIC_SCRATCH_BYTES that every GPU
  * loading this library holds until exit; grids whose planes are larger are
  * rejected with CB2_EINVAL.  No cudaMalloc / cudaFree or allocating routine
@@ -130,8 +145,9 @@ int cb2_run_bit_planes_at(int automaton, void* const* a, void* const* b, int64_t
  * before any stream capture.  All calls on a device share the array, so
  * calls that overlap on the GPU (different streams, or different host
  * threads) race; serialise them. */
-int cb2_run_bit_planes_in_place(int automaton, void* const* planes, int64_t x_size, int64_t y_size, int64_t steps,
-                                const cb2_tuning* tuning, void* stream);
+int cb2_run_bit_planes_in_place(int automaton, void* const* planes, int64_t x_size, int64_t y_size,
+                                int64_t time_step, int64_t steps, uint64_t seed, const cb2_tuning* tuning,
+                                void* stream);
 
 /* ---- owning device grids -------------------------------------------------- */
 /* A device-resident grid: P bit-planes, double-buffered, generation counter.
@@ -199,6 +215,34 @@ int cb2_band_pass(int automaton, void* const* in, void* const* out, int64_t x_si
 int cb2_band_pass_at(int automaton, void* const* in, void* const* out, int64_t x_size, int64_t rows_total,
                      int64_t row_first, int64_t rows_out, int temporal_steps, int64_t time_step, uint64_t seed,
                      int64_t global_row0, int64_t global_rows, const cb2_tuning* tuning, void* stream);
+/* Depths of the passes a band run of `steps` generations takes: passes of
+ * min(temporal_steps, ghost) generations, then the binary digits of the
+ * remainder from the largest down (45 steps at depth 32: 32, 8, 4, 1).
+ * Writes up to `capacity` depths and returns the number of passes (which may
+ * exceed capacity), or CB2_EINVAL.  Host only: needs no GPU. */
+int64_t cb2_band_schedule(int64_t steps, int temporal_steps, int ghost, int* depths, int64_t capacity);
+/* Fills this rank's ghost rows for the next pass: the `k` rows above its
+ * band (planes rows ghost-k .. ghost-1) from the last k band rows of the rank
+ * above, the k rows below (rows ghost+band .. ghost+band+k-1) from the first
+ * k band rows of the rank below, in buffer `buffer` (0: a, 1: b) of
+ * cb2_band_run, enqueued on `stream` (NCCL send/recv, peer copies, or plain
+ * copies for a single rank).  Returns 0, or a nonzero code that stops the run. */
+typedef int (*cb2_halo_exchange_fn)(void* user, int buffer, int k, void* stream);
+/* A whole band run for C and C++ hosts: `steps` generations from
+ * `time_step`, in passes of cb2_band_schedule's depths, alternating between
+ * the caller's buffers a and b (band_rows + 2 * ghost rows each, the band's
+ * first row being global row `global_row0` of `global_rows`).  Each pass
+ * overlaps the halo exchange with the band's interior: once the previous
+ * pass is done, `exchange` is enqueued on `exchange_stream` while the rows
+ * that need no ghost row (all but k at each edge) advance on `stream`; the
+ * two k-row edges follow once the exchange has landed.  Bands thinner than
+ * 3k rows run whole after the exchange.  Launches only; *result_in_b says
+ * which buffer holds the result.  The reference runs one grid on one GPU
+ * (traversers/cuda/temporal.cuh:153-245); this is its multi-GPU split. */
+int cb2_band_run(int automaton, void* const* a, void* const* b, int64_t x_size, int64_t band_rows, int ghost,
+                 int64_t time_step, int64_t steps, uint64_t seed, int64_t global_row0, int64_t global_rows,
+                 const cb2_tuning* tuning, cb2_halo_exchange_fn exchange, void* user, void* stream,
+                 void* exchange_stream, int* result_in_b);
 /* Seeded input (cb2_grid_fill_random's stream) for caller-owned planes whose
  * row y is global row (global_row0 + y) mod global_rows of the global grid. */
 int cb2_fill_random_planes(int automaton, void* const* planes, int64_t x_size, int64_t rows, int64_t global_row0,

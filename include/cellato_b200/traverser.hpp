@@ -15,6 +15,12 @@
 //   cellato_b200::suites::using_<word>::bit_planes<automaton> (and friends)
 //       suite types to list in suites_for (test_suites.hpp:259-285).
 //
+// The library holds precompiled rules looked up by the config's name; init()
+// also compares the config's fingerprint (cellato_b200/fingerprint.hpp: its
+// algorithm type and state dictionary) with the one the library registered
+// under that name, so a config that reuses a registered name with another
+// rule is rejected (std::invalid_argument) rather than run with the wrong one.
+//
 // Errors are rethrown with the reference's exception conventions
 // (traversers/cuda_utils.cuh:37-47, traversers/cuda/temporal.hpp:57-83):
 // CUDA failures as cellato_b200::cuda_error (a std::runtime_error),
@@ -22,7 +28,9 @@
 // std::invalid_argument, cells outside the dictionary as std::out_of_range.
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -39,6 +47,7 @@
 #include "cellato/memory/tiled_bit_planes_grid.hpp"
 
 #include "cellato_b200.h"
+#include "cellato_b200/fingerprint.hpp"
 
 namespace cellato_b200 {
 
@@ -176,6 +185,20 @@ public:
         if (id < 0)
             throw std::invalid_argument(std::string("automaton '") + automaton::name +
                                         "' has no network in the B200 backend");
+        uint64_t registered = 0;
+        check(cb2_automaton_fingerprint(id, &registered), "cb2_automaton_fingerprint");
+        constexpr uint64_t mine = fingerprint::of<automaton>();
+        if (registered != mine) {
+            char hex[64];
+            std::snprintf(hex, sizeof hex, "%016llx, registered %016llx", (unsigned long long)mine,
+                          (unsigned long long)registered);
+            throw std::invalid_argument(std::string("automaton '") + automaton::name +
+                                        "': this config's rule or state dictionary differs from the one the B200 "
+                                        "library registered under that name (fingerprint " + hex +
+                                        "); build the config into the library under a name of its own "
+                                        "(make -C cellato_b200/csrc USER_AUTOMATA=...)");
+        }
+        _id = id;
         _x = layout::x(grid);
         _y = layout::y(grid);
         const int k = params.temporal_steps;
@@ -195,18 +218,24 @@ public:
     struct no_callback {};
 
     // Advances `steps` generations.  With a callback, it is called with
-    // (iteration, host grid) before the first and after every step, like the
-    // reference's traversers (cpu/simple.hpp:51-80).
+    // (generations done, host grid) before the first pass and after every
+    // pass of the run's plan (temporal_steps generations, the last pass the
+    // remainder), as the reference's temporal traverser calls back once per
+    // chunk of temporal_steps (traversers/cuda/temporal.cuh:205-232).
     template <typename callback = no_callback>
     void run(int steps, callback&& callback_func = no_callback{}) {
         if (!_grid) throw std::logic_error("run() before init()");
         if constexpr (std::is_same_v<std::decay_t<callback>, no_callback>) {
             check(cb2_grid_run(_grid.get(), steps, &_tuning, nullptr), "cb2_grid_run");
         } else {
+            cb2_tuning plan{};
+            check(cb2_plan(_id, _x, _y, &_tuning, &plan), "cb2_plan");
             callback_func(0, current());
-            for (int s = 0; s < steps; ++s) {
-                check(cb2_grid_run(_grid.get(), 1, nullptr, nullptr), "cb2_grid_run");
-                callback_func(s + 1, current());
+            for (int done = 0; done < steps;) {
+                const int n = std::min(plan.temporal_steps, steps - done);
+                check(cb2_grid_run(_grid.get(), n, &_tuning, nullptr), "cb2_grid_run");
+                done += n;
+                callback_func(done, current());
             }
         }
     }
@@ -219,8 +248,7 @@ public:
 
 private:
     grid_t current() const {
-        const int64_t bytes =
-            cb2_layout_bytes(cb2_automaton_lookup(automaton::name), layout::layout, layout::word_bits, _x, _y);
+        const int64_t bytes = cb2_layout_bytes(_id, layout::layout, layout::word_bits, _x, _y);
         check((int)(bytes < 0 ? bytes : 0), "cb2_layout_bytes");
         std::vector<uint8_t> img((std::size_t)bytes);
         check(cb2_grid_download(_grid.get(), layout::layout, layout::word_bits, img.data(), img.size(), nullptr),
@@ -229,6 +257,7 @@ private:
     }
 
     std::unique_ptr<cb2_grid, detail::grid_deleter> _grid;
+    int _id = -1;
     int64_t _x = 0, _y = 0;
     cb2_tuning _tuning{0, 0, 0, 0};
 };

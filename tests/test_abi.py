@@ -25,7 +25,7 @@ def test_header_constants_match_binding():
 
 
 def test_abi_version():
-    assert _abi.lib.cb2_abi_version() == 3
+    assert _abi.lib.cb2_abi_version() == 4
 
 
 def test_automaton_registry():

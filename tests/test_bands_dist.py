@@ -1,9 +1,10 @@
 """Row bands across ranks, on CPU with gloo (world sizes 2 and 3): the halo
-exchange (cellato_b200.bands.exchange_halos, the code the GPU ranks run over
-NCCL) and the whole band decomposition -- exchange, then K generations per
-band -- against the oracle on the global grid.  The per-band stepping here
-is the oracle on the padded band (test infrastructure); on GPUs it is
-cb2_band_pass."""
+exchange (cellato_b200.bands.post_halos / exchange_halos, the code the GPU
+ranks run over NCCL) and the whole band run -- BandGrid.run's pass schedule
+(cb2_band_schedule), with the exchange posted before the band interior and
+completed before the two edges -- against the oracle on the global grid.
+Only the kernel is replaced: each pass is computed by the oracle on the
+window of rows it reads (test infrastructure); on GPUs it is cb2_band_pass_at."""
 import os
 import socket
 
@@ -56,40 +57,87 @@ def test_exchange_halos_gloo(world):
     assert [out[r] for r in range(world)] == [1] * world
 
 
+def _oracle_band_grid(automaton, x, rows, rank, world, ghost):
+    """A BandGrid on CPU tensors whose pass is the oracle instead of the kernel."""
+    from cellato_b200.bands import BandGrid
+    from oracle import oracle as O
+
+    class OracleBands(BandGrid):
+        def _pass(self, src, dst, row_first, rows_out, k, time_step, tuning, stream):
+            lo, hi = row_first - k, row_first + rows_out + k  # the rows a pass of k generations reads
+            window = src[:, lo:hi, :].contiguous().numpy().view(np.uint8).reshape(-1)
+            cells = O.unpack("bit_planes", window, x, hi - lo, self.P, 32)
+            nxt = O.run_standard(self.automaton, cells, k)  # rows within k of the window's edges are junk
+            new = O.pack("bit_planes", nxt, self.P, 32).view(np.int32).reshape(self.P, hi - lo, x // 32)
+            dst[:, row_first:row_first + rows_out] = torch.from_numpy(new[:, k:k + rows_out].copy())
+
+    return OracleBands(automaton, x, rows, rank=rank, world=world, ghost=ghost, device=torch.device("cpu"))
+
+
 def _bands_worker(rank, world, port, automaton, x, rows, steps, k, ghost, out):
     _init(rank, world, port)
-    from cellato_b200.bands import exchange_halos
     from oracle import oracle as O
     probs = {0: [0.5, 0.5], 1: [0.6, 0.05, 0.05, 0.3], 2: [0.125] * 8}[automaton]
     P = O.PLANES[automaton]
     cells = O.init_cells(x, rows, 99, O.thresholds(probs))
-    band = rows // world
-    row0 = rank * band
-    idx = [(row0 - ghost + i) % rows for i in range(band + 2 * ghost)]
-    padded = cells[idx]
-    planes = torch.from_numpy(O.pack("bit_planes", padded, P, 32).view(np.int32).reshape(P, band + 2 * ghost, x // 32).copy())
-    left = steps
-    while left > 0:
-        kk = min(k, left)
-        exchange_halos(planes, ghost, band, kk, rank, world)
-        cur = O.unpack("bit_planes", planes.numpy().view(np.uint8).reshape(-1), x, band + 2 * ghost, P, 32)
-        nxt = O.run_standard(automaton, cur, kk)  # ghost rows beyond kk are junk, never used
-        new = torch.from_numpy(O.pack("bit_planes", nxt, P, 32).view(np.int32).reshape(P, band + 2 * ghost, x // 32))
-        planes[:, ghost:ghost + band] = new[:, ghost:ghost + band]
-        left -= kk
-    mine = O.unpack("bit_planes", planes[:, ghost:ghost + band].contiguous().numpy().view(np.uint8).reshape(-1),
-                    x, band, P, 32)
+    b = _oracle_band_grid(automaton, x, rows, rank, world, ghost)
+    idx = [(b.row0 - ghost + i) % rows for i in range(b.rows_total)]
+    b.planes.copy_(torch.from_numpy(O.pack("bit_planes", cells[idx], P, 32).view(np.int32)
+                                    .reshape(P, b.rows_total, x // 32)))
+    passes = b.run(steps, temporal_steps=k)
+    mine = O.unpack("bit_planes", b.planes[:, ghost:ghost + b.band].contiguous().numpy().view(np.uint8).reshape(-1),
+                    x, b.band, P, 32)
     gathered = [torch.zeros_like(torch.from_numpy(mine)) for _ in range(world)]
     dist.all_gather(gathered, torch.from_numpy(mine.copy()))
     if rank == 0:
         full = np.concatenate([g.numpy() for g in gathered], axis=0)
         out["ok"] = bool((full == O.run_standard(automaton, cells, steps)).all())
+        out["passes"] = passes
     dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world,automaton", [(2, 0), (3, 1), (2, 2)])
-def test_band_decomposition_matches_global_oracle(world, automaton):
+@pytest.mark.parametrize("world,automaton,k", [(2, 0, 4), (3, 1, 4), (2, 2, 8), (3, 0, 16)])
+def test_band_run_matches_global_oracle(world, automaton, k):
+    # Bands of 24 rows: k = 4 and 8 take the interior/edge split, k = 16 the
+    # whole-band pass after the exchange; 21 steps end with remainder passes.
     out = mp.Manager().dict()
-    mp.spawn(_bands_worker, args=(world, _free_port(), automaton, 64, 24 * world, 21, 4, 5, out), nprocs=world,
+    ghost = max(5, k)
+    mp.spawn(_bands_worker, args=(world, _free_port(), automaton, 64, 24 * world, 21, k, ghost, out), nprocs=world,
              join=True)
     assert out["ok"]
+    assert out["passes"] == len(_schedule(21, k, ghost))
+
+
+def _schedule(steps, k, ghost):
+    import sys
+    sys.path.insert(0, ROOT)
+    from cellato_b200.bands import schedule
+    return schedule(steps, k, ghost)
+
+
+def test_band_schedule():
+    assert _schedule(45, 32, 32) == [32, 8, 4, 1]
+    assert _schedule(64, 32, 16) == [16, 16, 16, 16]
+    assert _schedule(0, 8, 32) == []
+    assert _schedule(7, 1, 32) == [1] * 7
+    from cellato_b200 import _abi
+    assert _abi.lib.cb2_band_schedule(5, 0, 32, None, 0) == _abi.CB2_EINVAL
+
+
+def _checksum_worker(rank, world, port, out):
+    _init(rank, world, port)
+    from cellato_b200.bands import BandGrid
+    b = BandGrid(0, 64, 32 * world, rank=rank, world=world, ghost=4, device=torch.device("cpu"))
+    # Sums modulo 2^64 (negative state values wrap, as the reference's
+    # uint64 sums do) must survive the int64 all-reduce.
+    big = [(1 << 64) - 5 - i if i % 2 else (1 << 63) + i for i in range(16)]
+    b.local_checksum = lambda values=None: list(big)
+    out[rank] = b.checksum()
+    dist.destroy_process_group()
+
+
+def test_band_checksum_sums_modulo_2_64():
+    out = mp.Manager().dict()
+    mp.spawn(_checksum_worker, args=(2, _free_port(), out), nprocs=2, join=True)
+    want = [(2 * ((1 << 64) - 5 - i if i % 2 else (1 << 63) + i)) % (1 << 64) for i in range(16)]
+    assert out[0] == want and out[1] == want

@@ -9,6 +9,21 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 EXE = os.path.join(ROOT, "cellato_b200", "_build", "dropin_check")
+FP_EXE = os.path.join(ROOT, "cellato_b200", "_build", "fingerprint_check")
+
+
+def test_dropin_binds_configs_by_type_not_name():
+    # A config that reuses a registered name with another rule (HighLife as
+    # "game-of-life", WireWorld with a reordered dictionary) is rejected by
+    # traverser::init before any device call; every bundled config's
+    # fingerprint equals the library's.  Needs no GPU.
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "tests", "native")], check=True)
+    if not os.path.exists(FP_EXE):
+        pytest.skip("neither the reference sources nor a prebuilt fingerprint_check")
+    r = subprocess.run([FP_EXE], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "fingerprints ok" in r.stdout
+    assert r.stdout.count("rejected:") == 2
 
 
 def test_dropin_builds_and_fails_cleanly_without_a_gpu():
