@@ -52,6 +52,25 @@ CB2_HD uint32_t east_of(uint32_t c, uint32_t right) {
 #endif
 }
 
+// One three-input logic operation with truth table LUT: bit i of LUT is the
+// result for a = bit 2 of i, b = bit 1, c = bit 0 (a = 0xF0, b = 0xCC,
+// c = 0xAA give LUT back).  On the device it is emitted as one lop3.b32, so
+// a network written with it keeps the operation count it is written with;
+// the host evaluates the same table.
+template <unsigned LUT>
+CB2_HD uint32_t lop3(uint32_t a, uint32_t b, uint32_t c) {
+#if defined(__CUDA_ARCH__)
+    uint32_t d;
+    asm("lop3.b32 %0, %1, %2, %3, %4;" : "=r"(d) : "r"(a), "r"(b), "r"(c), "n"(LUT));
+    return d;
+#else
+    uint32_t d = 0;
+    for (unsigned i = 0; i < 8; ++i)
+        if ((LUT >> i) & 1u) d |= ((i & 4u) ? a : ~a) & ((i & 2u) ? b : ~b) & ((i & 1u) ? c : ~c);
+    return d;
+#endif
+}
+
 CB2_HD uint32_t xor3(uint32_t a, uint32_t b, uint32_t c) { return a ^ b ^ c; }
 CB2_HD uint32_t maj3(uint32_t a, uint32_t b, uint32_t c) { return (a & b) | (c & (a | b)); }
 
@@ -90,26 +109,37 @@ struct game_of_life {
     }
 };
 
-// WireWorld, P = 2 (empty=0, head=1, tail=2, conductor=3).
+// WireWorld, P = 2 (empty=0, head=1, tail=2, conductor=3).  Ten LOP3 and
+// two funnel shifts per word and generation, each written as one lop3.
 struct wire {
     static constexpr int P = 2;
     static constexpr int NH = 2;
     static constexpr int id = 1;
     static constexpr bool kWindow = false;
-    CB2_HD static uint32_t indicator(const uint32_t (&s)[P]) { return s[0] & ~s[1]; }  // head
+    // head: s0 & ~s1
+    CB2_HD static uint32_t indicator(const uint32_t (&s)[P]) { return lop3<0x30>(s[0], s[1], s[0]); }
+    // the row's head count over (x-1, x, x+1) as two bits: xor3 and majority
     CB2_HD static void hagg(uint32_t l, uint32_t c, uint32_t r, uint32_t (&h)[NH]) {
-        h[0] = xor3(l, c, r);
-        h[1] = maj3(l, c, r);
+        h[0] = lop3<0x96>(l, c, r);
+        h[1] = lop3<0xE8>(l, c, r);
     }
     // head->tail, tail->conductor, conductor->head iff 1..2 head neighbours,
-    // empty->empty.  A conductor centre has T <= 8, so bit 3 cannot alias 1/2.
+    // empty->empty.  With the three rows' counts a, m, b (0..3 each) the 3x3
+    // count is S = p0 + 2*k0 + 2*x + 4*y for p0 = a0^m0^b0, k0 = maj(a0, m0,
+    // b0), x = a1^m1^b1, y = maj(a1, m1, b1); the centre is included, which is
+    // exact because only a conductor centre reads the count and it is not a
+    // head.  S is 1 or 2 iff y == 0 and (p0 ? k0 == x == 0 : k0 != x).
     CB2_HD static void next(const uint32_t (&a)[NH], const uint32_t (&m)[NH], const uint32_t (&b)[NH],
                             const uint32_t (&c)[P], uint32_t (&o)[P]) {
-        uint32_t t0, t1, t2;
-        census_sum(a, m, b, t0, t1, t2);
-        uint32_t one_or_two = (t0 ^ t1) & ~t2;
+        const uint32_t p0 = lop3<0x96>(a[0], m[0], b[0]);
+        const uint32_t k0 = lop3<0xE8>(a[0], m[0], b[0]);
+        const uint32_t x = lop3<0x96>(a[1], m[1], b[1]);
+        const uint32_t y = lop3<0xE8>(a[1], m[1], b[1]);
+        const uint32_t g = lop3<0x16>(p0, k0, x);      // p0 ? ~k0 & ~x : k0 ^ x
+        const uint32_t one_or_two = lop3<0x30>(g, y, g);  // g & ~y
         o[0] = c[1];
-        o[1] = (c[0] ^ c[1]) | (c[0] & c[1] & ~one_or_two);
+        // (c0 ^ c1) | (c0 & c1 & ~one_or_two): head -> tail (2), tail -> conductor (3), conductor -> 1 or 3
+        o[1] = lop3<0x7C>(c[0], c[1], one_or_two);
     }
 };
 
