@@ -18,7 +18,19 @@ e2e       the same metric through the C-ABI with host buffers: every step
 roofline  the strip kernel against the measured integer-logic peak (the
           binding roof for k >= 2) and against the measured HBM copy peak.
 cpu_baseline  Cellato's own CPU traverser (oracle/_ref, compiled from the
-          reference headers) on the host cores, on a bounded sample.
+          reference headers) on the benchmark grid itself, on the host cores:
+          all threads (each on a band of the grid's rows) and one thread (the
+          whole grid), over a timed sub-range of the step's generations.
+workloads  (one GPU) the WireWorld and Greenberg-Hastings 32768^2 x 2000
+          workloads, each with its own roofline, e2e and clocks.
+temporal_depths  (one GPU) the headline at k = 1, 2, 4, 8 generations per
+          HBM round trip, each with its fastest kernel, beside the autotuned k.
+batched, served, batched_dsl, served_dsl  many grids in one persistent kernel,
+          and continuous-batching serving, each against one grid at a time.
+
+--impl reference times Cellato's CPU traverser on the same grid on all host
+threads (each step a timed sub-range of the step's generations) and prints
+the same metric for the same config.
 """
 from __future__ import annotations
 
@@ -37,15 +49,15 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
-    "gol-65536": dict(automaton=0, x=65536, y=65536, gens=1000, probs=[0.65, 0.35], seed=42,
+    "gol-65536": dict(automaton=0, name="game-of-life", planes=1, x=65536, y=65536, gens=1000, probs=[0.65, 0.35], seed=42,
                       desc="game-of-life 65536x65536 bit_planes, Bernoulli(0.35), 1000 generations per step"),
-    "wire-32768": dict(automaton=1, x=32768, y=32768, gens=2000, probs=[0.60, 0.05, 0.05, 0.30], seed=42,
+    "wire-32768": dict(automaton=1, name="wire", planes=2, x=32768, y=32768, gens=2000, probs=[0.60, 0.05, 0.05, 0.30], seed=42,
                        desc="wire 32768x32768 bit_planes (2 planes), categorical "
                             "(empty .60, head .05, tail .05, conductor .30), 2000 generations per step"),
-    "excitable-32768": dict(automaton=2, x=32768, y=32768, gens=2000, probs=[0.125] * 8, seed=42,
+    "excitable-32768": dict(automaton=2, name="excitable", planes=3, x=32768, y=32768, gens=2000, probs=[0.125] * 8, seed=42,
                             desc="excitable (Greenberg-Hastings, 8 states) 32768x32768 bit_planes (3 planes), "
                                  "uniform states, 2000 generations per step"),
-    "gol-1024": dict(automaton=0, x=1024, y=1024, gens=100, probs=[0.5, 0.5], seed=42,
+    "gol-1024": dict(automaton=0, name="game-of-life", planes=1, x=1024, y=1024, gens=100, probs=[0.5, 0.5], seed=42,
                      desc="game-of-life 1024x1024, Bernoulli(0.5), 100 generations per step"),
 }
 METRIC = "Gcell-updates/s"
@@ -114,51 +126,117 @@ def gpu_index(local_rank: int) -> int:
 
 # ---- CPU baseline: Cellato's own CPU traverser ------------------------------------------------
 
-def cpu_sample(automaton: int, probs, target_s: float, threads: int | None = None) -> dict:
-    """Times the reference CPU simple traverser (bit_planes, 64-bit words) with
-    one independent grid per host thread on a 4096x4096 sample."""
-    from oracle import oracle as O
+def headline_config(wl, world: int) -> dict:
+    """The workload description both arms report (so the lines compare like for like)."""
+    x, y = wl["x"], wl["y"]
+    P = wl["planes"]
+    return {"workload": wl["desc"] + (f"; {world} row bands of {y} rows (one {x}x{y * world} grid)"
+                                      if world > 1 else ""),
+            "automaton": wl["name"], "x_size": x, "y_size": y * world, "generations_per_step": wl["gens"],
+            "seed": wl["seed"], "state_probabilities": wl["probs"],
+            "l2": (f"inputs larger than L2: each of the {P} plane(s) of each buffer is {x * y // 8 // 2**20} MiB "
+                   f"per GPU; every K-generation pass streams all of them"),
+            "parallelism": (f"row bands x{world}, NCCL halo exchange of K rows each way per pass" if world > 1
+                            else "single GPU")}
 
-    threads = threads or os.cpu_count() or 1
-    x = y = 4096
-    cells = O.init_cells(x, y, 1, O.thresholds(probs))
-    if O.ref_available():
-        kind = "reference"
-        run = lambda gens: O.ref_bench(automaton, cells, gens, threads, "bit_planes", 64)  # noqa: E731
-    else:  # the C restatement, single-threaded
-        kind, threads = "port", 1
-        planes = O.pack("bit_planes", cells, O.PLANES[automaton], 32).view("uint32")
 
-        def run(gens):
-            t0 = time.perf_counter()
-            O.run_bit_planes(automaton, planes, x, y, gens)
-            return time.perf_counter() - t0
-    probe = max(run(2), 1e-4)
-    gens = max(2, int(target_s / probe * 2))
-    secs = run(gens)
-    value = threads * x * y * gens / secs / 1e9
-    return {"value": value, "unit": METRIC, "cores": threads, "kind": kind,
-            "sample": f"{threads} host thread(s), each its own {x}x{y} grid, {gens} generations, "
-                      f"Cellato CPU simple traverser, bit_planes layout, 64-bit words ({secs:.2f} s)"}
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def host_threads(rows: int) -> int:
+    """Host threads for the CPU samples: all cores, rounded down to a divisor of the rows."""
+    n = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    return max(t for t in range(1, n + 1) if rows % t == 0)
+
+
+class ReferenceSample:
+    """Cellato's own CPU simple traverser (bit_planes layout, 64-bit words;
+    oracle/_ref, compiled from the reference headers) on the benchmark's grid
+    itself: the seeded input built as bit planes, then advanced (a) by all
+    host threads, each on its band of rows of the grid as a torus of its own,
+    so that every cell of the grid advances once per generation, and (b) by
+    one thread over the whole grid.  Without the reference build, the oracle's
+    C restatement (single-threaded, whole grid) stands in."""
+
+    def __init__(self, wl, world: int):
+        from oracle import oracle as O
+
+        self.O = O
+        self.a, self.x, self.y, self.gens = wl["automaton"], wl["x"], wl["y"] * world, wl["gens"]
+        self.P = O.PLANES[self.a]
+        self.threads = host_threads(self.y)
+        t0 = time.perf_counter()
+        self.planes = O.init_bit_planes(self.x, self.y, self.P, wl["seed"], O.thresholds(wl["probs"]),
+                                        threads=self.threads)
+        self.init_s = time.perf_counter() - t0
+        self.kind = "reference" if O.ref_available() else "port"
+        if self.kind == "port":
+            self.threads = 1
+
+    def time(self, gens: int, threads: int) -> float:
+        if self.kind == "reference":
+            return self.O.ref_bench_planes64(self.a, self.planes, self.x, self.y, gens, threads)
+        t0 = time.perf_counter()
+        self.O.run_bit_planes(self.a, self.planes.reshape(-1), self.x, self.y, gens)
+        return time.perf_counter() - t0
+
+    def sample(self, target_s: float, threads: int) -> dict:
+        probe = max(self.time(1, threads), 1e-4)
+        gens = max(1, min(self.gens, int(target_s / probe)))
+        secs = self.time(gens, threads)
+        return {"value": self.x * self.y * gens / secs / 1e9, "gens": gens, "secs": secs, "threads": threads}
+
+    def describe(self, s: dict) -> str:
+        where = (f"{s['threads']} host threads, each the reference traverser on a {self.x}x{self.y // s['threads']} "
+                 f"band of the {self.x}x{self.y} grid (a torus of its own)" if s["threads"] > 1 else
+                 f"1 host thread, the whole {self.x}x{self.y} grid")
+        what = ("Cellato CPU simple traverser, bit_planes layout, 64-bit words" if self.kind == "reference" else
+                "C restatement of the bit-plane evaluator (oracle port)")
+        full_s = s["secs"] * self.gens / s["gens"]
+        return (f"{where}; {what}; {s['gens']} of the step's {self.gens} generations timed ({s['secs']:.2f} s), "
+                f"a full step extrapolated at that rate to {full_s:.1f} s; host CPU {cpu_model()}")
+
+    def baseline(self, target_s: float) -> dict:
+        """cpu_baseline of the B200 arm: the all-threads aggregate, and one thread."""
+        agg = self.sample(target_s, self.threads)
+        one = self.sample(min(target_s, 4.0), 1) if self.threads > 1 else agg
+        return {"value": agg["value"], "unit": METRIC, "cores": agg["threads"], "kind": self.kind,
+                "sample": self.describe(agg),
+                "single_core": {"value": one["value"], "unit": METRIC, "cores": 1, "sample": self.describe(one)},
+                "cpu_model": cpu_model()}
 
 
 def reference_arm(args, wl) -> None:
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    target = 8.0
-    samples = []
+    ref = ReferenceSample(wl, world)
     for _ in range(args.warmup):
-        cpu_sample(wl["automaton"], wl["probs"], 1.0)
-    for _ in range(args.steps):
-        samples.append(cpu_sample(wl["automaton"], wl["probs"], target))
-    value = statistics.mean(s["value"] for s in samples)
-    base = dict(samples[-1])
-    base["value"] = value
+        ref.sample(0.5, ref.threads)
+    samples = [ref.sample(2.0, ref.threads) for _ in range(args.steps)]
+    gens = sum(s["gens"] for s in samples)
+    secs = sum(s["secs"] for s in samples)
+    value = ref.x * ref.y * gens / secs / 1e9
+    one = ref.sample(2.0, 1) if ref.threads > 1 else samples[-1]
+    base = {"value": value, "unit": METRIC, "cores": ref.threads, "kind": ref.kind,
+            "sample": ref.describe(dict(samples[-1], gens=gens, secs=secs)),
+            "single_core": {"value": one["value"], "unit": METRIC, "cores": 1, "sample": ref.describe(one)},
+            "cpu_model": cpu_model()}
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-           "config": {"workload": wl["desc"], "sample": base["sample"]},
+           "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": secs / gens * ref.gens * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+           "config": headline_config(wl, world),
+           "sample": (f"each step times {samples[-1]['gens']} generations of the step's {ref.gens} on the "
+                      f"benchmark grid; ms_per_step extrapolates the measured rate to the whole step"),
            "cpu_baseline": base, "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
                                          "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
@@ -338,6 +416,188 @@ def launches_per_run(gens: int, k: int) -> int:
     return n
 
 
+class Ranks:
+    """Barrier and max-over-ranks for the timed regions (no-ops on one rank)."""
+
+    def __init__(self, torch, dist, world: int):
+        self.torch, self.dist, self.world = torch, dist, world
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, v: float) -> float:
+        if self.world == 1:
+            return v
+        t = self.torch.tensor([v], dtype=self.torch.float64, device="cuda")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+
+def roofline(cb, a, name, x, y, P, plan, avg_launch_s, gens_per_launch, lop3_peak, traffic_key=True) -> dict:
+    """The strip kernel against the measured integer-logic peak and the measured HBM copy peak."""
+    cells = x * y
+    bytes_per_launch = 2 * P * cells / 8  # read + write every plane once
+    hbm_gbs = bytes_per_launch / avg_launch_s / 1e9
+    peaks = measured_peaks()
+    hbm_peak = peaks.get("hbm_gbs", FALLBACK_HBM_GBS)
+    alu_per_word, shfl_per_word = cb.network_ops(a)
+    int_gops = alu_per_word * (cells / 32) * gens_per_launch / avg_launch_s / 1e9
+    int_frac = int_gops / (lop3_peak / 1e9)
+    hbm_frac = hbm_gbs / hbm_peak
+    key = (f"pipe_kernel<{name},K={plan['temporal_steps']},V={plan['words_per_lane']},L={plan['levels_per_warp']},"
+           f"R={plan['rows_per_step']}>@{x}x{y}")
+    is_int = int_frac >= hbm_frac
+    return {
+        "bound": "int" if is_int else "hbm",
+        "kernel": key,
+        "achieved": int_gops if is_int else hbm_gbs,
+        "peak": lop3_peak / 1e9 if is_int else hbm_peak,
+        "unit": "Gop/s" if is_int else "GB/s",
+        "frac": max(int_frac, hbm_frac),
+        "traffic": traffic_for(key) if traffic_key else None,
+        "peak_source": ("measured LOP3 issue rate (cb2_measure_lop3_peak, this run)" if is_int else
+                        ("measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback 6.65 TB/s")),
+        "int": {"achieved_gops": int_gops, "peak_gops": lop3_peak / 1e9, "frac": int_frac,
+                "ops_per_word_per_generation": alu_per_word, "shuffles_per_word_per_generation": shfl_per_word},
+        "hbm": {"achieved_gbs": hbm_gbs, "peak_gbs": hbm_peak, "frac": hbm_frac,
+                "algorithmic_bytes_per_launch": bytes_per_launch,
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
+        "avg_launch_ms": avg_launch_s * 1e3,
+        "generations_per_launch": gens_per_launch,
+    }
+
+
+def best_plan_for_depth(cb, torch, grid, a, x, y, k: int, stream) -> dict:
+    """Autotuning at a fixed temporal depth: every instantiated strip kernel of
+    depth k, timed over 64 generations on the grid itself; the fastest plan."""
+    best, best_ms = None, None
+    for (kk, v, lv, r) in cb.variants(a):
+        if kk != k:
+            continue
+        plan = dict(temporal_steps=k, words_per_lane=v, levels_per_warp=lv, rows_per_step=r)
+        grid.run(k, **plan, stream=stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        grid.run(64, **plan, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        if best_ms is None or ms < best_ms:
+            best, best_ms = plan, ms
+    return best
+
+
+def measure(cb, torch, ranks, wl, args, rank, world, local_rank, stream, lop3_peak, depth: int = 0,
+            e2e: bool = True) -> dict:
+    """Times `args.steps` steps of workload `wl` (after `args.warmup` warm-up
+    steps) with inputs resident in HBM, and, with `e2e`, the same steps through
+    the public API with the bit planes copied from and to pinned host memory.
+    depth > 0 fixes the temporal depth (the fastest kernel of that depth)."""
+    a, x, y, gens = wl["automaton"], wl["x"], wl["y"], wl["gens"]
+    name, P, _ = cb.automaton_info(a)
+    cells = x * y
+    tuned = None
+    if world == 1:
+        grid = cb.DeviceGrid(a, x, y)
+        grid.fill_random(wl["seed"], wl["probs"], stream=stream)
+        if depth:
+            run_kw = best_plan_for_depth(cb, torch, grid, a, x, y, depth, stream)
+            grid.fill_random(wl["seed"], wl["probs"], stream=stream)
+        else:
+            tuned = None if args.no_autotune else cb.autotune(a, x, y, budget_ms=4000)
+            run_kw = {}
+        plan = cb.plan(a, x, y, **run_kw)
+    else:
+        # one grid of world*y rows split into bands, one per rank (NCCL halo exchange per pass)
+        from cellato_b200.bands import BandGrid
+
+        if not args.no_autotune:
+            tuned = cb.autotune(a, x, y, budget_ms=4000)
+        grid = BandGrid(a, x, y * world, rank, world)
+        grid.fill_random(wl["seed"], wl["probs"], stream=stream)
+        # every rank must take the same passes (one halo exchange each): use rank 0's depth
+        kt = torch.tensor([depth or grid.plan_k()], dtype=torch.int64, device="cuda")
+        ranks.dist.broadcast(kt, 0)
+        run_kw = {"temporal_steps": int(kt.item())}
+        plan = cb.plan(a, x, y, **run_kw)
+    k = plan["temporal_steps"]
+
+    # ---- device-resident timing ----
+    for _ in range(args.warmup):
+        grid.run(gens, **run_kw, stream=stream)
+    torch.cuda.synchronize()
+    ranks.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(gpu_index(local_rank)) if local_rank == 0 else None
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        grid.run(gens, **run_kw, stream=stream)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    ranks.barrier()
+    clocks = sampler.stop() if sampler else None
+    ms = ranks.max(e0.elapsed_time(e1))
+    value = world * cells * gens * args.steps / (ms * 1e-3) / 1e9
+    launches = launches_per_run(gens, k) * args.steps * (1 if world == 1 else 3)
+    strip_launches = launches_per_run(gens, k) * args.steps
+    roof = roofline(cb, a, name, x, y, P, plan, ms * 1e-3 / strip_launches, gens * args.steps / strip_launches,
+                    lop3_peak)
+    out = {"value": value, "unit": METRIC, "ms_per_step": ms / args.steps, "plan": plan, "autotuned": tuned,
+           "roofline": roof, "clocks": clocks, "gpu_launches": launches}
+
+    if e2e:
+        nbytes = cb.layout_bytes(a, "bit_planes", 64, x, y)
+        host_in = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+        host_out = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+        if world == 1:
+            grid.download("bit_planes", 64, stream=stream, out=host_in.numpy())
+            host_img = cb.HostGrid(a, "bit_planes", 64, x, y, host_in.numpy())
+
+            def e2e_step():
+                grid.upload(host_img, stream=stream)
+                grid.run(gens, **run_kw, stream=stream)
+                grid.download("bit_planes", 64, stream=stream, out=host_out.numpy())
+        else:
+            g0, nb = grid.ghost, grid.band
+            band_in = host_in.view(torch.int32).view(P, nb, x // 32)
+            band_out = host_out.view(torch.int32).view(P, nb, x // 32)
+            band_in.copy_(grid.planes[:, g0:g0 + nb])
+
+            def e2e_step():
+                grid.planes[:, g0:g0 + nb].copy_(band_in, non_blocking=True)
+                grid.run(gens, **run_kw, stream=stream)
+                band_out.copy_(grid.planes[:, g0:g0 + nb], non_blocking=True)
+                torch.cuda.current_stream().synchronize()
+        e2e_step()
+        torch.cuda.synchronize()
+        ranks.barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        w0 = time.perf_counter()
+        f0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        f1.record(stream)
+        f1.synchronize()
+        wall = time.perf_counter() - w0
+        ranks.barrier()
+        e2e_ms = ranks.max(f0.elapsed_time(f1))
+        out["e2e"] = {"value": world * cells * gens * args.steps / (e2e_ms * 1e-3) / 1e9, "unit": METRIC,
+                      "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "wall_s": ranks.max(wall),
+                      "path": ("cb2_grid_upload(bit_planes) + cb2_grid_run + cb2_grid_download, pinned host buffers"
+                               if world == 1 else "band planes from pinned host memory + BandGrid.run (halo "
+                                                  "exchange overlapped with the band interior, cb2_band_pass_at "
+                                                  "per pass) + band planes back, per rank")}
+    if world == 1:
+        grid.close()
+    else:
+        del grid
+    torch.cuda.synchronize()
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -352,6 +612,8 @@ def main() -> None:
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-extra-workloads", action="store_true",
+                    help="skip the WireWorld / Greenberg-Hastings lines and the per-depth lines")
     ap.add_argument("--serve-requests", type=int, default=300)
     ap.add_argument("--serve-dsl-requests", type=int, default=300,
                     help="requests of the served point over the lowered DSL automata (0 = skip)")
@@ -376,139 +638,29 @@ def main() -> None:
 
     import cellato_b200 as cb
 
-    a, x, y, gens = wl["automaton"], wl["x"], wl["y"], wl["gens"]
-    name, P, _ = cb.automaton_info(a)
-    cells = x * y
+    ranks = Ranks(torch, dist, world)
     stream = torch.cuda.current_stream()
-    tuned = None if args.no_autotune else cb.autotune(a, x, y, budget_ms=4000)
-    plan = cb.plan(a, x, y)
-    k = plan["temporal_steps"]
-    if world == 1:
-        grid = cb.DeviceGrid(a, x, y)
-        grid.fill_random(wl["seed"], wl["probs"], stream=stream)
-    else:
-        # one grid of world*y rows split into bands, one per rank (NCCL halo exchange per pass)
-        from cellato_b200.bands import BandGrid
-
-        grid = BandGrid(a, x, y * world, rank, world)
-        grid.fill_random(wl["seed"], wl["probs"], stream=stream)
-        # every rank must take the same passes (one halo exchange each): use rank 0's depth
-        kt = torch.tensor([grid.plan_k()], dtype=torch.int64, device="cuda")
-        dist.broadcast(kt, 0)
-        k = int(kt.item())
-
-    run_kw = {} if world == 1 else {"temporal_steps": k}
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    # ---- device-resident timing ----
-    for _ in range(args.warmup):
-        grid.run(gens, **run_kw, stream=stream)
-    torch.cuda.synchronize()
-    barrier()
-    torch.cuda.synchronize()
-    sampler = ClockSampler(gpu_index(local_rank)) if local_rank == 0 else None
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        grid.run(gens, **run_kw, stream=stream)
-    e1.record(stream)
-    e1.synchronize()
-    torch.cuda.synchronize()
-    barrier()
-    clocks = sampler.stop() if sampler else None
-    ms = max_over_ranks(e0.elapsed_time(e1))
-    value = world * cells * gens * args.steps / (ms * 1e-3) / 1e9
-    launches = launches_per_run(gens, k) * args.steps
-
-    # ---- roofline of the strip kernel ----
-    avg_launch_s = ms * 1e-3 / launches
-    gens_per_launch = gens * args.steps / launches
-    bytes_per_launch = 2 * P * cells / 8  # read + write every plane once
-    hbm_gbs = bytes_per_launch / avg_launch_s / 1e9
-    peaks = measured_peaks()
-    hbm_peak = peaks.get("hbm_gbs", FALLBACK_HBM_GBS)
     lop3_peak = cb.measure_lop3_peak()
-    alu_per_word, shfl_per_word = cb.network_ops(a)
-    int_ops_per_launch = alu_per_word * (cells / 32) * gens_per_launch
-    int_gops = int_ops_per_launch / avg_launch_s / 1e9
-    int_frac = int_gops / (lop3_peak / 1e9)
-    hbm_frac = hbm_gbs / hbm_peak
-    kernel_key = (f"pipe_kernel<{name},K={k},V={plan['words_per_lane']},L={plan['levels_per_warp']},"
-                  f"R={plan['rows_per_step']}>@{x}x{y}")
-    traffic = traffic_for(kernel_key)
-    roof = {
-        "bound": "int" if int_frac >= hbm_frac else "hbm",
-        "kernel": kernel_key,
-        "achieved": int_gops if int_frac >= hbm_frac else hbm_gbs,
-        "peak": lop3_peak / 1e9 if int_frac >= hbm_frac else hbm_peak,
-        "unit": "Gop/s" if int_frac >= hbm_frac else "GB/s",
-        "frac": max(int_frac, hbm_frac),
-        "traffic": traffic,
-        "peak_source": ("measured LOP3 issue rate (cb2_measure_lop3_peak, this run)" if int_frac >= hbm_frac else
-                        ("measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback 6.65 TB/s")),
-        "int": {"achieved_gops": int_gops, "peak_gops": lop3_peak / 1e9, "frac": int_frac,
-                "ops_per_word_per_generation": alu_per_word, "shuffles_per_word_per_generation": shfl_per_word},
-        "hbm": {"achieved_gbs": hbm_gbs, "peak_gbs": hbm_peak, "frac": hbm_frac,
-                "algorithmic_bytes_per_launch": bytes_per_launch,
-                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
-        "avg_launch_ms": avg_launch_s * 1e3,
-        "generations_per_launch": gens_per_launch,
-    }
+    head = measure(cb, torch, ranks, wl, args, rank, world, local_rank, stream, lop3_peak)
 
-    # ---- end to end through the public API with host buffers ----
-    nbytes = cb.layout_bytes(a, "bit_planes", 64, x, y)
-    host_in = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
-    host_out = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
-    if world == 1:
-        grid.download("bit_planes", 64, stream=stream, out=host_in.numpy())
-        host_img = cb.HostGrid(a, "bit_planes", 64, x, y, host_in.numpy())
+    # BASELINE's other single-grid configs, and the headline at each fixed temporal depth
+    workloads, depths = None, None
+    if world == 1 and not args.no_extra_workloads and args.workload == "gol-65536":
+        workloads = {}
+        for key in ("wire-32768", "excitable-32768"):
+            workloads[key] = dict(measure(cb, torch, ranks, WORKLOADS[key], args, rank, world, local_rank, stream,
+                                          lop3_peak), workload=WORKLOADS[key]["desc"])
+        depth_args = argparse.Namespace(**dict(vars(args), steps=max(2, min(args.steps, 5)), warmup=3))
+        depths = {"workload": wl["desc"], "steps": depth_args.steps, "warmup": depth_args.warmup,
+                  "note": "each depth runs its fastest strip kernel, timed on the grid itself (autotuned per k)",
+                  "autotuned": {"temporal_steps": head["plan"]["temporal_steps"], "value": head["value"],
+                                "roofline_frac": head["roofline"]["frac"], "bound": head["roofline"]["bound"]}}
+        for k in (1, 2, 4, 8):
+            r = measure(cb, torch, ranks, wl, depth_args, rank, world, local_rank, stream, lop3_peak, depth=k,
+                        e2e=False)
+            depths[f"k={k}"] = {"value": r["value"], "unit": METRIC, "ms_per_step": r["ms_per_step"],
+                                "plan": r["plan"], "roofline": r["roofline"], "clocks": r["clocks"]}
 
-        def e2e_step():
-            grid.upload(host_img, stream=stream)
-            grid.run(gens, **run_kw, stream=stream)
-            grid.download("bit_planes", 64, stream=stream, out=host_out.numpy())
-    else:
-        g0, nb = grid.ghost, grid.band
-        band_in = host_in.view(torch.int32).view(P, nb, x // 32)
-        band_out = host_out.view(torch.int32).view(P, nb, x // 32)
-        band_in.copy_(grid.planes[:, g0:g0 + nb])
-
-        def e2e_step():
-            grid.planes[:, g0:g0 + nb].copy_(band_in, non_blocking=True)
-            grid.run(gens, **run_kw, stream=stream)
-            band_out.copy_(grid.planes[:, g0:g0 + nb], non_blocking=True)
-            torch.cuda.current_stream().synchronize()
-    e2e_step()
-    torch.cuda.synchronize()
-    barrier()
-    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    w0 = time.perf_counter()
-    f0.record(stream)
-    for _ in range(args.steps):
-        e2e_step()
-    f1.record(stream)
-    f1.synchronize()
-    wall = time.perf_counter() - w0
-    barrier()
-    e2e_ms = max_over_ranks(f0.elapsed_time(f1))
-    e2e_wall = max_over_ranks(wall)
-    e2e_value = world * cells * gens * args.steps / (e2e_ms * 1e-3) / 1e9
-
-    if world == 1:
-        grid.close()
-    else:
-        del grid
-    torch.cuda.synchronize()
     batched = None
     if not args.no_batch:
         batched = bench_batch(cb, torch, stream, args.batch_grids, max(3, args.steps))
@@ -524,7 +676,7 @@ def main() -> None:
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_sample(a, wl["probs"], args.cpu_seconds)
+        cpu = ReferenceSample(wl, world).baseline(args.cpu_seconds)
 
     if world > 1:
         dist.barrier()
@@ -532,24 +684,18 @@ def main() -> None:
     if rank != 0:
         return
     out = {
-        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": head["value"], "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": wl["desc"], "automaton": name, "x_size": x, "y_size": y,
-                   "generations_per_step": gens, "plan": plan, "autotuned": tuned,
-                   "l2": (f"inputs larger than L2: each of the {P} plane(s) of each buffer is "
-                          f"{x * y // 8 // 2**20} MiB at {x}x{y}; a K-generation pass streams all of them"),
-                   "parallelism": (f"row bands x{world}: one {x}x{y * world} grid, {y} rows per GPU, NCCL halo "
-                                   f"exchange of K rows each way per pass" if world > 1 else "single GPU")},
-        "roofline": roof,
-        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-                "wall_s": e2e_wall,
-                "path": ("cb2_grid_upload(bit_planes) + cb2_grid_run + cb2_grid_download, pinned host buffers"
-                         if world == 1 else "band planes from pinned host memory + BandGrid.run (halo exchange + "
-                                            "cb2_band_pass per pass) + band planes back, per rank")},
-        "gpu_launches": launches,
-        "clocks": clocks,
+        "config": headline_config(wl, world),
+        "plan": head["plan"], "autotuned": head["autotuned"],
+        "roofline": head["roofline"],
+        "e2e": head["e2e"],
+        "gpu_launches": head["gpu_launches"],
+        "clocks": head["clocks"],
         "cpu_baseline": cpu,
+        "workloads": workloads,
+        "temporal_depths": depths,
         "batched": batched,
         "batched_dsl": batched_dsl,
         "served": served,
