@@ -295,7 +295,8 @@ def batch_probs(cb, a):
     return [0.5, 0.25, 0.25] if states == 3 else [1.0 / states] * states  # exact binary fractions
 
 
-def bench_batch(cb, torch, stream, n: int, runs: int, automata=(0, 1, 2)) -> dict:
+def bench_batch(cb, torch, stream, n: int, runs: int, automata=(0, 1, 2), temporal_steps: int = 0,
+                tile_rows: int = 0) -> dict:
     specs = batch_workload(n, automata=automata)
     grids = []
     for i, (a, x, y, _) in enumerate(specs):
@@ -304,7 +305,7 @@ def bench_batch(cb, torch, stream, n: int, runs: int, automata=(0, 1, 2)) -> dic
         g.set_seed(5000 + i)
         grids.append(g)
     steps = [s for (_, _, _, s) in specs]
-    batch = cb.Batch(grids, steps)
+    batch = cb.Batch(grids, steps, temporal_steps=temporal_steps, tile_rows=tile_rows)
     info = batch.info()
     for _ in range(2):
         batch.run(stream)
@@ -333,6 +334,7 @@ def bench_batch(cb, torch, stream, n: int, runs: int, automata=(0, 1, 2)) -> dic
                         f"{{{names}}}, steps log-uniform [10,1000], seeded inits",
             "value": cells / (ms * 1e-3) / 1e9, "unit": METRIC, "ms_per_run": ms, "runs": runs,
             "cell_updates_per_run": cells, "tasks": info["tasks"], "persistent_ctas": info["persistent_ctas"],
+            "chunk_generations": temporal_steps or "library default", "tile_rows": tile_rows or "library default",
             "per_grid_value": cells / (per_ms * 1e-3) / 1e9, "per_grid_ms_per_run": per_ms,
             "speedup_vs_per_grid": per_ms / ms,
             "path": "cb2_batch_run (persistent tile-queue kernel, CUDA graph replay) vs cb2_batch_run_per_grid "

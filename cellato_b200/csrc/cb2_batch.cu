@@ -65,10 +65,13 @@
 namespace cb2 {
 
 constexpr int kBuiltinPlanes = 3;  // the hand-written networks' largest P
+constexpr int kBatchDefaultK = 32;      // cb2_batch_create's chunk length (capped at kBatchKMax with lowered rules)
+constexpr int kBatchDefaultRows = 768;  // and its tile height for the hand-written networks
 constexpr int kBuiltinRows = 4;    // rows each warp passes on per barrier (2: 18.3, 4: 19.1, 8: 16.6 Tcell/s)
 
-// The hand-written networks: the kernel of kind kBatchBuiltin.  KMAX = 4
-// drops the eight-generation pipelines (a batch whose chunks are at most 4).
+// The hand-written networks: the kernel of kind kBatchBuiltin, one per
+// longest chunk KMAX (4, 8, 16 or 32 generations), so that a batch of short
+// chunks does not carry the registers of the longer pipelines.
 template <int KMAX>
 struct builtin_rules {
     static constexpr int kWarps = kBatchKindWarps[kBatchBuiltin];
@@ -102,6 +105,8 @@ __global__ void batch_flip_kernel(batch_grid_desc* grids, const unsigned char* o
 
 static const void* batch_kernel_for(int kind, int kmax) {
     if (kind == kBatchAll) return generic_batch_kernel();
+    if (kmax >= 32) return (const void*)batch_kernel<builtin_rules<32>>;
+    if (kmax >= 16) return (const void*)batch_kernel<builtin_rules<16>>;
     return kmax >= 8 ? (const void*)batch_kernel<builtin_rules<8>> : (const void*)batch_kernel<builtin_rules<4>>;
 }
 
@@ -119,7 +124,7 @@ static int ecuda(cudaError_t e, const char* what) {
 }
 
 int batch_engine::init(int task_capacity, int grid_capacity, int kmax_, long long spin_limit_) {
-    kmax = kmax_ >= 8 ? 8 : 4;
+    kmax = kmax_ >= 32 ? 32 : kmax_ >= 16 ? 16 : (kmax_ >= 8 ? 8 : 4);
     spin_limit = spin_limit_ > 0 ? spin_limit_ : (1ll << 23);
     task_cap = std::max(1, task_capacity);
     grid_cap = std::max(1, grid_capacity);
@@ -177,12 +182,16 @@ int batch_engine::build(const std::vector<batch_item>& items, const batch_tiling
     std::vector<plan_t> plans((size_t)n);
     std::vector<int> order((size_t)n);
     kind = kBatchBuiltin;
+    for (const batch_item& it : items)
+        if (it.grid->g.automaton >= kNumBuiltin) kind = kBatchAll;
+    // the kernel over every automaton runs chunks of at most kBatchKMax
+    const int kcap = kind == kBatchAll ? std::min(kmax, kBatchKMax) : kmax;
     for (int i = 0; i < n; ++i) {
         const batch_item& it = items[(size_t)i];
         const cb2_grid* g = it.grid;
         plan_t& p = plans[(size_t)i];
         int64_t left = it.steps;
-        const int kmain = std::min(kmax, tiling.temporal_steps > 0 ? tiling.temporal_steps : kmax);
+        const int kmain = std::min(kcap, tiling.temporal_steps > 0 ? tiling.temporal_steps : kcap);
         if (it.steps / kmain > INT_MAX) return efail(CB2_EINVAL, "too many generations for one batch run");
         while (left > 0) {
             int k = kmain;
@@ -217,7 +226,6 @@ int batch_engine::build(const std::vector<batch_item>& items, const batch_tiling
         d.kmain = kmain;
         d.nfull = (int32_t)(it.steps / kmain);
         d.rem = (int32_t)(it.steps % kmain);
-        if (d.automaton >= kNumBuiltin) kind = kBatchAll;
         h_odd[i] = (unsigned char)(p.ks.size() & 1);
         order[(size_t)i] = i;
     }
@@ -370,12 +378,18 @@ int cb2_batch_create(cb2_grid* const* grids, const int64_t* steps, int n, const 
     cb2_batch_opts o{0, 0, 0, -1};
     if (opts) o = *opts;
     if (o.temporal_steps && o.temporal_steps != 1 && o.temporal_steps != 2 && o.temporal_steps != 4 &&
-        o.temporal_steps != 8)
-        return efail(CB2_EINVAL, "batch temporal_steps must be 1, 2, 4 or 8");
+        o.temporal_steps != 8 && o.temporal_steps != 16 && o.temporal_steps != 32)
+        return efail(CB2_EINVAL, "batch temporal_steps must be 1, 2, 4, 8, 16 or 32");
     auto* b = new cb2_batch();
-    b->tiling.temporal_steps = o.temporal_steps ? o.temporal_steps : 8;
-    b->tiling.tile_rows = o.tile_rows > 0 ? o.tile_rows : 256;
+    // Defaults measured on the batched workload (4096 mixed network grids):
+    // chunks of 8 generations and 256-row tiles 20.5 Tcell/s, 16 and 512 rows
+    // 21.4, 32 and 512 rows 23.5, 32 and 768 rows 23.9, 32 and 1024 rows 22.7.
+    b->tiling.temporal_steps = o.temporal_steps ? o.temporal_steps : kBatchDefaultK;
+    b->tiling.tile_rows = o.tile_rows > 0 ? o.tile_rows : kBatchDefaultRows;
     b->tiling.lowered_tile_rows = o.tile_rows > 0 ? o.tile_rows : 64;
+    bool lowered = false;  // a lowered DSL automaton caps every chunk of the batch at kBatchKMax
+    for (int i = 0; i < n; ++i) lowered = lowered || (grids[i] && grids[i]->g.automaton >= kNumBuiltin);
+    const int kchunk = lowered ? std::min(b->tiling.temporal_steps, kBatchKMax) : b->tiling.temporal_steps;
     int64_t est = 0;
     for (int i = 0; i < n; ++i) {
         if (!grids[i] || steps[i] < 0) {
@@ -384,7 +398,7 @@ int cb2_batch_create(cb2_grid* const* grids, const int64_t* steps, int n, const 
         }
         b->items.push_back(batch_item{grids[i], steps[i], grids[i]->cur, grids[i]->time_step, grids[i]->seed});
         const cb2_grid* g = grids[i];
-        const int64_t chunks = steps[i] / std::max(1, b->tiling.temporal_steps) + 4;
+        const int64_t chunks = steps[i] / std::max(1, kchunk) + 6;
         const int64_t rows = std::max<int64_t>(1, std::min<int64_t>(g->g.h, b->tiling.rows_for(g->g.automaton)));
         const int64_t per_chunk =
             g->g.wd <= 16 ? (g->g.h + 1) / 2 + 1 : ((g->g.h + rows - 1) / rows) * ((g->g.wd + 29) / 30);

@@ -16,7 +16,7 @@
 
 namespace cb2 {
 
-constexpr int kBatchKMax = 8;  // longest chunk of a task
+constexpr int kBatchKMax = 8;  // longest chunk of a task of the kernel over every automaton
 
 // Input rows a task keeps in flight: at least two groups of `rows`.
 __host__ __device__ constexpr int batch_ring_depth(int rows) { return 2 * rows > kRingDepth ? 2 * rows : kRingDepth; }
@@ -76,15 +76,21 @@ __device__ __forceinline__ void batch_run_task(const strip_task& t, const lane_g
         pipe_rows_idle<K, L, ROWS>(t);
 }
 
-// One task of rule R with the chunk length k of the task (1, 2, 4, or KMAX).
+// One task of rule R with the chunk length k of the task (1, 2, 4, 8, 16 or 32, up to KMAX).
 template <class R, int KMAX, int ROWS, int SMEM, int WARPS>
 __device__ __forceinline__ void batch_run_rule(const strip_task& t, int k, const lane_geom<1>& geom, uint32_t* smem) {
     switch (k) {
     case 1: batch_run_task<R, 1, ROWS, SMEM, WARPS>(t, geom, smem); break;
     case 2: batch_run_task<R, 2, ROWS, SMEM, WARPS>(t, geom, smem); break;
     case 4: batch_run_task<R, 4, ROWS, SMEM, WARPS>(t, geom, smem); break;
-    default:
+    case 8:
         if constexpr (KMAX >= 8) batch_run_task<R, 8, ROWS, SMEM, WARPS>(t, geom, smem);
+        break;
+    case 16:
+        if constexpr (KMAX >= 16) batch_run_task<R, 16, ROWS, SMEM, WARPS>(t, geom, smem);
+        break;
+    default:
+        if constexpr (KMAX >= 32) batch_run_task<R, 32, ROWS, SMEM, WARPS>(t, geom, smem);
         break;
     }
 }

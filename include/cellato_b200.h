@@ -272,8 +272,9 @@ int cb2_checksum_planes(int automaton, const void* const* planes, int64_t x_size
 typedef struct cb2_batch cb2_batch;
 
 typedef struct cb2_batch_opts {
-    int temporal_steps;   /* K of full chunks: 1, 2, 4 or 8 (0 = 8)                  */
-    int tile_rows;        /* output rows per strip task (0 = 256 for the hand-written
+    int temporal_steps;   /* K of full chunks: 1, 2, 4, 8, 16 or 32 (0 = 32; batches
+                             holding a lowered DSL automaton run chunks of at most 8) */
+    int tile_rows;        /* output rows per strip task (0 = 768 for the hand-written
                              networks, 64 for lowered DSL rules)                       */
     long long spin_limit; /* iterations a task waits for its grid's previous chunk
                              before the run fails with CB2_ETIMEOUT (0 = ~4 s)         */
@@ -308,8 +309,9 @@ typedef struct cb2_server_opts {
     size_t memory_budget;    /* bytes of request state held at once (0 = min(150 GiB, 80% free)) */
     int max_active;          /* requests admitted at once (0 = 4096)                    */
     int chunk_steps;         /* most generations per request per round (0 = 128)       */
-    int temporal_steps;      /* K of the batch kernel: 1, 2, 4 or 8 (0 = 8)            */
-    int tile_rows;           /* output rows per strip task (0 = 128 for the hand-written
+    int temporal_steps;      /* K of the batch kernel: 1, 2, 4, 8, 16 or 32 (0 = 32;
+                                rounds holding a lowered DSL request use at most 8)  */
+    int tile_rows;           /* output rows per strip task (0 = 256 for the hand-written
                                 networks, 64 for lowered DSL rules)                    */
     int per_request;         /* 1 = plain one-request-at-a-time path                   */
     int task_capacity;       /* strip tasks per round (0 = 2^20)                        */

@@ -75,3 +75,11 @@ def test_tuning_file_round_trip(tmp_path):
 def test_network_op_counts():
     alu, shf = cb.network_ops("game-of-life")
     assert alu == 12 and shf == 1
+
+
+def test_server_rejects_unsupported_chunk_lengths():
+    # checked before any device call: the batch kernel has pipelines of 1, 2, 4, 8, 16 and 32 generations only
+    opts = _abi.ServerOpts(0, 0, 0, 12, 0, 0, 0, 0, 0, 0.0, 0)
+    h = ctypes.c_void_p()
+    assert _abi.lib.cb2_server_create(ctypes.byref(opts), ctypes.byref(h)) == _abi.CB2_EINVAL
+    assert "temporal_steps" in _abi.last_error()

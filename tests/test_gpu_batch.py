@@ -95,7 +95,9 @@ def test_stalled_dependency_times_out_and_the_context_survives(cuda):
     # the kernel records it and every warp stops; the host sees TimeoutError.
     specs = [(0, 256, 64), (1, 128, 64)]
     grids, cells = make_grids(specs, 400)
-    with cb.Batch(grids, [16, 16], spin_limit=2000, stall_task=3) as b:
+    # chunks of 8: two chunks per grid, one task each, so task 3 is grid 1's second chunk
+    with cb.Batch(grids, [16, 16], temporal_steps=8, spin_limit=2000, stall_task=3) as b:
+        assert b.info()["tasks"] == 4
         b.run()
         with pytest.raises(TimeoutError, match="spin limit"):
             b.wait()
