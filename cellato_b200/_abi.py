@@ -132,6 +132,8 @@ _SIGNATURES = {
     "cb2_grid_destroy": (ctypes.c_int, [_vp]),
     "cb2_grid_upload": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_size_t, _vp]),
     "cb2_grid_download": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_size_t, _vp]),
+    "cb2_grid_upload_async": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_size_t, _vp]),
+    "cb2_grid_download_async": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_size_t, _vp]),
     "cb2_layout_bytes": (_i64, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _i64, _i64]),
     "cb2_grid_fill_random": (ctypes.c_int, [_vp, ctypes.c_uint64, _u64p, ctypes.c_int, _vp]),
     "cb2_grid_run": (ctypes.c_int, [_vp, _i64, _tp, _vp]),

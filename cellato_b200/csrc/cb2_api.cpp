@@ -389,14 +389,14 @@ static int ensure_staging(cb2_grid* grid, size_t bytes) {
     return CB2_OK;
 }
 
-int cb2_grid_upload(cb2_grid* grid, int layout, int word_bits, const void* host, size_t bytes, void* stream) {
+// Enqueues the upload of a host image (copy, and the layout conversion) on s.
+static int enqueue_upload(cb2_grid* grid, int layout, int word_bits, const void* host, size_t bytes, cudaStream_t s) {
     if (!grid || !host) return fail(CB2_EINVAL, "null grid or host pointer");
     const grid_geom& g = grid->g;
     const int64_t need = cb2_layout_bytes(g.automaton, layout, word_bits, g.x_size, g.y_size);
     if (need < 0) return (int)need;
     if ((int64_t)bytes != need)
         return fail(CB2_EINVAL, "host image is " + std::to_string(bytes) + " bytes, layout needs " + std::to_string(need));
-    cudaStream_t s = (cudaStream_t)stream;
     uint32_t* dst = grid->buf[grid->cur];
     if (layout == CB2_LAYOUT_BIT_PLANES ||
         (layout == CB2_LAYOUT_BIT_ARRAY && g.planes == 1)) {  // one plane: bit_array == bit_planes bytes
@@ -416,24 +416,37 @@ int cb2_grid_upload(cb2_grid* grid, int layout, int word_bits, const void* host,
         }
         if (e != cudaSuccess) return cuda_fail(e, "layout conversion launch");
     }
+    grid->time_step = 0;
+    return CB2_OK;
+}
+
+int cb2_grid_upload(cb2_grid* grid, int layout, int word_bits, const void* host, size_t bytes, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc = enqueue_upload(grid, layout, word_bits, host, bytes, s);
+    if (rc) return rc;
     CB2_CUDA(cudaStreamSynchronize(s));
     if (layout == CB2_LAYOUT_STANDARD) {
         unsigned bad = 0;
         CB2_CUDA(cudaMemcpy(&bad, grid->flag, sizeof(unsigned), cudaMemcpyDeviceToHost));
         if (bad) return fail(CB2_ESTATE, "State not found in dictionary (a cell value exceeds the automaton's states)");
     }
-    grid->time_step = 0;
     return CB2_OK;
 }
 
-int cb2_grid_download(cb2_grid* grid, int layout, int word_bits, void* host, size_t bytes, void* stream) {
+int cb2_grid_upload_async(cb2_grid* grid, int layout, int word_bits, const void* host, size_t bytes, void* stream) {
+    if (layout == CB2_LAYOUT_STANDARD)
+        return fail(CB2_EINVAL, "the standard layout's cells are checked on the host: use cb2_grid_upload");
+    return enqueue_upload(grid, layout, word_bits, host, bytes, (cudaStream_t)stream);
+}
+
+// Enqueues the download of the current generation (conversion, and copy) on s.
+static int enqueue_download(cb2_grid* grid, int layout, int word_bits, void* host, size_t bytes, cudaStream_t s) {
     if (!grid || !host) return fail(CB2_EINVAL, "null grid or host pointer");
     const grid_geom& g = grid->g;
     const int64_t need = cb2_layout_bytes(g.automaton, layout, word_bits, g.x_size, g.y_size);
     if (need < 0) return (int)need;
     if ((int64_t)bytes != need)
         return fail(CB2_EINVAL, "host image is " + std::to_string(bytes) + " bytes, layout needs " + std::to_string(need));
-    cudaStream_t s = (cudaStream_t)stream;
     const uint32_t* src = grid->buf[grid->cur];
     if (layout == CB2_LAYOUT_BIT_PLANES || (layout == CB2_LAYOUT_BIT_ARRAY && g.planes == 1)) {
         CB2_CUDA(cudaMemcpyAsync(host, src, bytes, cudaMemcpyDeviceToHost, s));
@@ -450,8 +463,19 @@ int cb2_grid_download(cb2_grid* grid, int layout, int word_bits, void* host, siz
         if (e != cudaSuccess) return cuda_fail(e, "layout conversion launch");
         CB2_CUDA(cudaMemcpyAsync(host, grid->staging, bytes, cudaMemcpyDeviceToHost, s));
     }
+    return CB2_OK;
+}
+
+int cb2_grid_download(cb2_grid* grid, int layout, int word_bits, void* host, size_t bytes, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc = enqueue_download(grid, layout, word_bits, host, bytes, s);
+    if (rc) return rc;
     CB2_CUDA(cudaStreamSynchronize(s));
     return CB2_OK;
+}
+
+int cb2_grid_download_async(cb2_grid* grid, int layout, int word_bits, void* host, size_t bytes, void* stream) {
+    return enqueue_download(grid, layout, word_bits, host, bytes, (cudaStream_t)stream);
 }
 
 int cb2_grid_fill_random(cb2_grid* grid, uint64_t seed, const uint64_t* thresholds, int n, void* stream) {

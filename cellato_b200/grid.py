@@ -181,6 +181,26 @@ class DeviceGrid:
                                   host.data.ctypes.data_as(ctypes.c_void_p), host.data.nbytes,
                                   _stream_handle(stream)), "upload")
 
+    def upload_async(self, host: HostGrid, stream=None) -> None:
+        """upload() enqueued on `stream` without waiting (cb2_grid_upload_async):
+        `host` must stay unchanged until the stream has passed the copy."""
+        if host.automaton != self.automaton or host.x_size != self.x_size or host.y_size != self.y_size:
+            raise ValueError("host grid does not match this device grid")
+        check(lib.cb2_grid_upload_async(self._h, _abi.LAYOUTS[host.layout], host.word_bits,
+                                        host.data.ctypes.data_as(ctypes.c_void_p), host.data.nbytes,
+                                        _stream_handle(stream)), "upload")
+
+    def download_async(self, out: np.ndarray, layout: str = "bit_planes", word_bits: int = 64, stream=None) -> None:
+        """download() into `out` enqueued on `stream` without waiting
+        (cb2_grid_download_async): `out` is written when the stream passes the copy."""
+        n = layout_bytes(self.automaton, layout, word_bits, self.x_size, self.y_size)
+        buf = out.view(np.uint8).reshape(-1)
+        if buf.nbytes != n:
+            raise ValueError(f"output buffer of {buf.nbytes} bytes, expected {n}")
+        check(lib.cb2_grid_download_async(self._h, _abi.LAYOUTS[layout], word_bits,
+                                          buf.ctypes.data_as(ctypes.c_void_p), n, _stream_handle(stream)),
+              "download")
+
     def upload_cells(self, cells: np.ndarray, stream=None) -> None:
         self.upload(HostGrid.from_cells(self.automaton, cells), stream)
 

@@ -167,6 +167,18 @@ int cb2_grid_destroy(cb2_grid* grid);
  * index.  Both calls complete the copy before returning. */
 int cb2_grid_upload(cb2_grid* grid, int layout, int word_bits, const void* host, size_t bytes, void* stream);
 int cb2_grid_download(cb2_grid* grid, int layout, int word_bits, void* host, size_t bytes, void* stream);
+/* The same copies enqueued on `stream` without waiting for them, so that a
+ * caller streaming a sequence of grids can overlap one grid's upload and
+ * another's download with a third's run (two copy streams and events).  No
+ * counterpart in the reference, whose traversers copy synchronously in init
+ * and fetch_result.  The host image must stay valid and unchanged (upload)
+ * or unread (download) until the stream has passed the copy; from pinned
+ * host memory the copy runs beside kernels.  A grid's upload, runs and
+ * download must still be ordered (one stream, or events).  The standard
+ * layout is refused by the upload (its cells are checked on the host:
+ * cb2_grid_upload). */
+int cb2_grid_upload_async(cb2_grid* grid, int layout, int word_bits, const void* host, size_t bytes, void* stream);
+int cb2_grid_download_async(cb2_grid* grid, int layout, int word_bits, void* host, size_t bytes, void* stream);
 /* Size of a layout's host image for a grid of this automaton and size. */
 int64_t cb2_layout_bytes(int automaton, int layout, int word_bits, int64_t x_size, int64_t y_size);
 

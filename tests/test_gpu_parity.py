@@ -252,3 +252,47 @@ def test_translation_invariance_large(cuda):
         base, _ = device_run(a, cells, steps)
         moved, _ = device_run(a, np.roll(cells, (777, 96), axis=(0, 1)), steps)
         assert (np.roll(base, (777, 96), axis=(0, 1)) == moved).all(), a
+
+
+def test_async_upload_download_pipeline(cuda):
+    # cb2_grid_upload_async / cb2_grid_download_async: three grids streamed
+    # through two device grids with two copy streams and events, as the
+    # bench's e2e leg does, give the synchronous path's results byte for byte.
+    torch = cuda
+    cases = [(0, 1024, 96, 37), (1, 2048, 64, 21), (2, 512, 160, 50), (0, 1024, 96, 12)]  # the last reuses grid 0
+    h2d, d2h, comp = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+    pinned_in, pinned_out, want = [], [], []
+    for i, (a, x, y, steps) in enumerate(cases):
+        cells = O.init_cells(x, y, 70 + i, O.thresholds(PROBS[a]))
+        n = cb.layout_bytes(a, "bit_planes", 64, x, y)
+        pi = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+        pi.numpy()[:] = O.pack("bit_planes", cells, O.PLANES[a], 64)
+        pinned_in.append(cb.HostGrid(a, "bit_planes", 64, x, y, pi.numpy()))
+        pinned_out.append(torch.empty(n, dtype=torch.uint8, pin_memory=True))
+        want.append(O.pack("bit_planes", O.run_standard(a, cells, steps), O.PLANES[a], 64))
+    slots = {}
+    downs = {}
+    for i, (a, x, y, steps) in enumerate(cases):
+        key = (a, x, y)
+        g = slots.setdefault(key, cb.DeviceGrid(a, x, y))
+        if key in downs:
+            h2d.wait_event(downs[key])
+        g.upload_async(pinned_in[i], stream=h2d)
+        up = torch.cuda.Event()
+        up.record(h2d)
+        comp.wait_event(up)
+        g.run(steps, stream=comp)
+        ran = torch.cuda.Event()
+        ran.record(comp)
+        d2h.wait_event(ran)
+        g.download_async(pinned_out[i].numpy(), stream=d2h)
+        downs[key] = torch.cuda.Event()
+        downs[key].record(d2h)
+    torch.cuda.synchronize()
+    for i in range(len(cases)):
+        assert pinned_out[i].numpy().tobytes() == want[i].tobytes(), i
+    g = next(iter(slots.values()))
+    with pytest.raises(ValueError, match="standard"):
+        g.upload_async(cb.HostGrid.from_cells(g.automaton, np.zeros((g.y_size, g.x_size), dtype=np.uint8)))
+    for g in slots.values():
+        g.close()
