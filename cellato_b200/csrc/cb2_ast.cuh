@@ -34,6 +34,12 @@
 //                              by (seed, S, generation, x / 64, y), sampled
 //                              exactly (core/probability.hpp:12-160)
 //
+// Evaluation is lazy where it pays: a branch of if_then_else, and the right
+// operand of and_ / or_, is evaluated with the mask of the cells where its
+// value is used (cell_ctx::care), and a probability draw resolves only those
+// cells.  A cell's draw depends on that cell's random bits alone, so every
+// used value is the reference's; values outside the mask are never read.
+//
 // The result of the rule is a state index; its low P bits are the new planes.
 #pragma once
 
@@ -255,6 +261,21 @@ __device__ __forceinline__ void ratio_digits(const uint32_t (&bits)[M], uint32_t
     }
 }
 
+// ratio_digits for digits J .. E-1 only.
+template <uint64_t n, uint64_t d, int J, int E, int M>
+__device__ __forceinline__ void ratio_digits_to(const uint32_t (&bits)[M], uint32_t& active, uint32_t& result) {
+    if constexpr (J < E) {
+        constexpr uint64_t r = rem_after(n, d, J);
+        if constexpr (r >= d - r) {
+            result |= active & ~bits[J];
+            active &= bits[J];
+        } else {
+            active &= ~bits[J];
+        }
+        ratio_digits_to<n, d, J + 1, E>(bits, active, result);
+    }
+}
+
 template <uint64_t Num, uint64_t Den>
 __device__ __forceinline__ uint32_t bernoulli_word(const cell_ctx& c, uint64_t lane) {
     static_assert(Den > 0 && Num <= Den, "a probability lies in [0, 1]");
@@ -268,6 +289,7 @@ __device__ __forceinline__ uint32_t bernoulli_word(const cell_ctx& c, uint64_t l
         if constexpr ((d & (d - 1)) == 0) {
             constexpr int M = dyadic_draws<n, d>();
             uint32_t draws[M + (M & 1)];
+            if (!__any_sync(kFullMask, c.care)) return 0u;  // no cell of the warp uses the draw
             if (c.paired) {  // warp-uniform
                 pair_stream s(lane, c);
 #pragma unroll
@@ -285,8 +307,12 @@ __device__ __forceinline__ uint32_t bernoulli_word(const cell_ctx& c, uint64_t l
             // time; draws past the one that resolves the last lane are not used.
             // A warp of 1024 cells needs about 11 digits, so a pair, whose shuffles
             // make the tail dearer, computes 12 up front (8: lightning-forest 0.99
-            // against 1.15 Tcell/s).
-            uint32_t active = 0xffffffffu, result = 0;
+            // against 1.15 Tcell/s).  Only the cells that use the draw
+            // (cell_ctx::care) need to leave the threshold; when none of the warp's
+            // is left after 10 digits, the last two are not drawn (lightning-forest
+            // at 16384^2: 0.96 -> 1.05 Tcell/s; a first check after 6 or 8 digits
+            // gained less, 1.00 and 1.03).
+            uint32_t active = c.care, result = 0;
             auto digit = [&](uint64_t& rem, uint32_t bits) {
                 if (rem >= d - rem) {
                     rem -= d - rem;
@@ -298,12 +324,17 @@ __device__ __forceinline__ uint32_t bernoulli_word(const cell_ctx& c, uint64_t l
                 }
             };
             if (c.paired) {  // warp-uniform: the pair's shuffles run on every lane
-                constexpr int kAhead = 12;
+                constexpr int kFirst = 10, kAhead = 12;
+                if (!__any_sync(kFullMask, active)) return 0u;
                 uint32_t ahead[kAhead];
                 pair_stream s(lane, c);
 #pragma unroll
-                for (int j = 0; j < kAhead; j += 2) s.next2(ahead[j], ahead[j + 1]);
-                ratio_digits<n, d, 0>(ahead, active, result);
+                for (int j = 0; j < kFirst; j += 2) s.next2(ahead[j], ahead[j + 1]);
+                ratio_digits_to<n, d, 0, kFirst>(ahead, active, result);
+                if (!__any_sync(kFullMask, active)) return result;
+#pragma unroll
+                for (int j = kFirst; j < kAhead; j += 2) s.next2(ahead[j], ahead[j + 1]);
+                ratio_digits_to<n, d, kFirst, kAhead>(ahead, active, result);
                 uint64_t rem = rem_after(n, d, kAhead);
                 while (__any_sync(kFullMask, active)) {
                     uint32_t d0, d1;
@@ -481,11 +512,16 @@ struct ev<Dict, A::less_than<L, R>> {
     }
 };
 
+// The right operand of and_ matters only where the left is true, of or_ only
+// where it is false.
 template <class Dict, class L, class R>
 struct ev<Dict, A::and_<L, R>> {
     template <int P>
     __device__ __forceinline__ static bv<1> eval(const window<P>& w, const cell_ctx& c) {
-        return mask(truth(ev<Dict, L>::eval(w, c)) & truth(ev<Dict, R>::eval(w, c)));
+        const uint32_t l = truth(ev<Dict, L>::eval(w, c));
+        cell_ctx cr = c;
+        cr.care = c.care & l;
+        return mask(l & truth(ev<Dict, R>::eval(w, cr)));
     }
 };
 
@@ -493,7 +529,10 @@ template <class Dict, class L, class R>
 struct ev<Dict, A::or_<L, R>> {
     template <int P>
     __device__ __forceinline__ static bv<1> eval(const window<P>& w, const cell_ctx& c) {
-        return mask(truth(ev<Dict, L>::eval(w, c)) | truth(ev<Dict, R>::eval(w, c)));
+        const uint32_t l = truth(ev<Dict, L>::eval(w, c));
+        cell_ctx cr = c;
+        cr.care = c.care & ~l;
+        return mask(l | truth(ev<Dict, R>::eval(w, cr)));
     }
 };
 
@@ -576,8 +615,11 @@ struct ev<Dict, A::if_then_else<C, T, E>> {
     template <int P>
     __device__ __forceinline__ static auto eval(const window<P>& w, const cell_ctx& c) {
         const uint32_t m = truth(ev<Dict, C>::eval(w, c));
-        const auto a = ev<Dict, T>::eval(w, c);
-        const auto b = ev<Dict, E>::eval(w, c);
+        cell_ctx ct = c, ce = c;  // each branch matters only where it is taken
+        ct.care = c.care & m;
+        ce.care = c.care & ~m;
+        const auto a = ev<Dict, T>::eval(w, ct);
+        const auto b = ev<Dict, E>::eval(w, ce);
         constexpr int N = max_of(sizeof(a.w) / 4, sizeof(b.w) / 4);
         const bv<N> x = resize<N>(a), y = resize<N>(b);
         bv<N> r;

@@ -62,6 +62,9 @@ struct cell_ctx {
     uint64_t seed;
     const uint64_t* key = nullptr;
     bool paired = false;
+    // The cells whose value of the node being evaluated is used; elsewhere
+    // the node may return anything (a probability draw resolves only these).
+    uint32_t care = 0xffffffffu;
 };
 
 // Where a row pushed into a level chain sits, for window rules (ast_rule):
