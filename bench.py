@@ -28,6 +28,9 @@ workloads  (one GPU) the WireWorld and Greenberg-Hastings 32768^2 x 2000
           workloads, each with its own roofline, e2e and clocks.
 temporal_depths  (one GPU) the headline at k = 1, 2, 4, 8 generations per
           HBM round trip, each with its fastest kernel, beside the autotuned k.
+layouts   (one GPU) the headline step through the bit_planes, bit_array and
+          tiled_bit_planes host layouts (conversions on the device at the
+          boundary), with the boundary's share of each step.
 batched, served, batched_dsl, served_dsl  many grids in one persistent kernel,
           and continuous-batching serving, each against one grid at a time.
 
@@ -547,6 +550,54 @@ def e2e_pipelined(cb, torch, grid, a, x, y, gens, run_kw, steps: int, stream) ->
                     "step i+1's upload and step i-1's download overlap step i's run"}
 
 
+def bench_layouts(cb, torch, wl, stream, steps: int = 3) -> dict:
+    """The headline step through each host layout a Cellato grid can have
+    (cb2_grid_upload / cb2_grid_download, synchronous, from and to pinned host
+    memory): the device always runs the linear bit planes, and the bit_array
+    and tiled_bit_planes images are converted on the device at upload and
+    download.  Per layout: ms per step (upload, 1000 generations, download)
+    and the boundary's share of it.  The standard layout (one byte per cell,
+    4 GiB at 65536^2) is left out."""
+    import numpy as np
+
+    a, x, y, gens = wl["automaton"], wl["x"], wl["y"], wl["gens"]
+    out = {"workload": wl["desc"], "steps": steps, "layouts": {}}
+    with cb.DeviceGrid(a, x, y) as g:
+        g.fill_random(wl["seed"], wl["probs"], stream=stream)
+        for layout in ("bit_planes", "bit_array", "tiled_bit_planes"):
+            n = cb.layout_bytes(a, layout, 64, x, y)
+            h_in = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+            h_out = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+            g.download(layout, 64, stream=stream, out=h_in.numpy())
+            img = cb.HostGrid(a, layout, 64, x, y, h_in.numpy())
+
+            def copies():
+                g.upload(img, stream=stream)
+                g.download(layout, 64, stream=stream, out=h_out.numpy())
+            copies()
+            torch.cuda.synchronize()
+            same = bool(np.array_equal(h_in.numpy(), h_out.numpy()))  # upload + download is the identity
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                copies()
+            io_ms = (time.perf_counter() - t0) * 1e3 / steps
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0 = time.perf_counter()
+            e0.record(stream)
+            for _ in range(steps):
+                g.upload(img, stream=stream)
+                g.run(gens, stream=stream)
+                g.download(layout, 64, stream=stream, out=h_out.numpy())
+            e1.record(stream)
+            e1.synchronize()
+            step_ms = e0.elapsed_time(e1) / steps
+            out["layouts"][layout] = {"ms_per_step": step_ms, "upload_download_ms": io_ms,
+                                      "boundary_share": io_ms / step_ms, "host_bytes": n,
+                                      "value": x * y * gens / (step_ms * 1e-3) / 1e9, "unit": METRIC,
+                                      "round_trip_equal": same}
+    return out
+
+
 def measure(cb, torch, ranks, wl, args, rank, world, local_rank, stream, lop3_peak, depth: int = 0,
             e2e: bool = True) -> dict:
     """Times `args.steps` steps of workload `wl` (after `args.warmup` warm-up
@@ -711,6 +762,10 @@ def main() -> None:
             depths[f"k={k}"] = {"value": r["value"], "unit": METRIC, "ms_per_step": r["ms_per_step"],
                                 "plan": r["plan"], "roofline": r["roofline"], "clocks": r["clocks"]}
 
+    layouts = None
+    if world == 1 and not args.no_extra_workloads and args.workload == "gol-65536":
+        layouts = bench_layouts(cb, torch, wl, stream)
+
     batched = None
     if not args.no_batch:
         batched = bench_batch(cb, torch, stream, args.batch_grids, max(3, args.steps))
@@ -746,6 +801,7 @@ def main() -> None:
         "cpu_baseline": cpu,
         "workloads": workloads,
         "temporal_depths": depths,
+        "layouts": layouts,
         "batched": batched,
         "batched_dsl": batched_dsl,
         "served": served,
