@@ -12,6 +12,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -137,6 +138,12 @@ int cb2_band_run(int automaton, void* const* a, void* const* b, int64_t x_size, 
         run_plan p;
         if ((rc = resolve_plan(band, &t0, &p))) return rc;
         k_main = p.k;
+    }
+    if (band_rows < std::min(k_main, ghost)) {
+        // the exchange copies the neighbours' first / last k band rows
+        set_error("bands of " + std::to_string(band_rows) + " rows are thinner than a pass of " +
+                  std::to_string(std::min(k_main, ghost)) + " generations");
+        return CB2_EINVAL;
     }
     const int64_t n = cb2_band_schedule(steps, k_main, ghost, nullptr, 0);
     if (n < 0) return (int)n;
