@@ -396,10 +396,11 @@ def bench_serve(cb, n: int, rates, automata=(0, 1, 2)) -> dict:
     serve_stream(cb, specs[:20], 1000.0, True)
     points = []
     for rate in rates:
-        # the median of three runs of the batched server (one Poisson stream each; the
-        # makespan is a few tenths of a second, so single runs vary by 10-20 %)
-        runs = sorted((serve_stream(cb, specs, rate, False) for _ in range(3)), key=lambda r: r["throughput"])
-        batched = dict(runs[1], throughput_of_runs=[r["throughput"] for r in runs])
+        # the median of five runs of the batched server (one Poisson stream each, the same
+        # arrival times; the makespan is a few tenths of a second and which requests share a
+        # round depends on host timing, so single runs vary, occasionally by 2x)
+        runs = sorted((serve_stream(cb, specs, rate, False) for _ in range(5)), key=lambda r: r["throughput"])
+        batched = dict(runs[2], throughput_of_runs=[r["throughput"] for r in runs])
         plain = serve_stream(cb, specs, rate, True)
         points.append({"rate_req_s": rate, "batched": batched, "per_request": plain,
                        "throughput_ratio": batched["throughput"] / plain["throughput"]})
