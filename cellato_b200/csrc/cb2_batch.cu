@@ -253,21 +253,32 @@ int batch_engine::build(const std::vector<batch_item>& items, const batch_tiling
             const int base = ntasks;
             const int h = items[(size_t)i].grid->g.h;
             const int span = p.groups ? p.rows * p.groups : p.rows;
+            // A last strip of at most 14 own words runs as row bands side by side
+            // in the warp (band_geom): floor(32 / (own words + 2)) of them, so that
+            // it fills the warp.  The bands split the tile's rows exactly, so a
+            // full tile takes a band count that divides its height.
+            const int rem_words = items[(size_t)i].grid->g.wd - 30 * (p.nsx - 1);
+            const int band_max = p.groups ? 1 : 32 / (rem_words + 2);
             for (int ty = 0; ty < p.nsy; ++ty) {
                 const int y0 = ty * span;
                 const bool last = ty == p.nsy - 1;
                 // the last tile row takes every remaining row
+                const int tile = last ? h - y0 : span;
                 const int rows = !last ? p.rows
                                  : p.groups ? (h - y0 + p.groups - 1) / p.groups
                                             : h - y0;
+                int bands = std::min(band_max, tile);
+                if (!last)
+                    while (tile % bands) --bands;
                 for (int tx = 0; tx < p.nsx; ++tx) {
+                    const bool banded = tx == p.nsx - 1 && bands > 1;
                     batch_task& t = h_tasks[ntasks++];
                     t.grid = i;
                     t.chunk = c;
                     t.dep_base = prev_base[(size_t)i];
-                    t.rows = rows;
+                    t.rows = banded ? (tile + bands - 1) / bands : rows;
                     t.k = (int16_t)p.ks[(size_t)c];
-                    t.groups = (int16_t)p.groups;
+                    t.groups = (int16_t)(banded ? -bands : p.groups);
                     t.nsx = (int16_t)p.nsx;
                     t.nsy = (int16_t)p.nsy;
                     t.tx = (int16_t)tx;

@@ -11,16 +11,18 @@
 
 namespace cb2 {
 
-// One CTA's work: one strip (groups == 0) or `groups` exact-wrap copies of a
-// narrow grid's row (groups > 0), for one chunk of k generations.  The tasks
-// of a chunk tile the grid as nsy rows of nsx tasks; (tx, ty) is this one.
+// One CTA's work: one strip (groups == 0), `groups` exact-wrap copies of a
+// narrow grid's row (groups > 0), or -groups row bands of a narrow last
+// strip side by side in the warp (groups < 0, band_geom), for one chunk of k
+// generations.  The tasks of a chunk tile the grid as nsy rows of nsx tasks;
+// (tx, ty) is this one.
 struct batch_task {
     int32_t grid;      // index into the grid table
     int32_t chunk;     // reads buffer chunk & 1, writes the other one
     int32_t dep_base;  // index of the previous chunk's first task, -1 for chunk 0
-    int32_t rows;      // output rows of the task (strip), or of each group
-    int16_t k;         // generations (1, 2, 4 or 8)
-    int16_t groups;    // 0 = strip task
+    int32_t rows;      // output rows of the task (strip), or of each group / band
+    int16_t k;         // generations (1 .. 32)
+    int16_t groups;    // 0 = strip task, > 0 exact-wrap groups, < 0 row bands
     int16_t nsx, nsy;  // tasks per tile row / tile rows of this grid's chunks
     int16_t tx, ty;    // this task's tile
     int32_t y0;        // first output row; the last tile row absorbs the remainder,

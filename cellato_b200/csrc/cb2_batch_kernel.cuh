@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(D::kWarps * 32) batch_kernel(batch_args a) {
         lane_geom<1> geom;
         st.y0 = task.y0;
         st.ny = task.rows;
-        if (task.groups) {
+        if (task.groups > 0) {
             st.x0 = 0;
             st.nx = gd.wd;
             geom = group_geom(st, task.groups, lane);
@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(D::kWarps * 32) batch_kernel(batch_args a) {
             const int shift = D::kTimed && gd.automaton >= kNumBuiltin ? 1 : 0;
             st.x0 = task.tx * 30 + shift;
             st.nx = min(30, gd.wd - task.tx * 30);
-            geom = strip_geom<1>(st, lane);
+            geom = task.groups < 0 ? band_geom(st, -task.groups, lane) : strip_geom<1>(st, lane);
         }
         D::run(gd.automaton, task.k, st, geom, smem);
         __threadfence();  // this thread's stores are visible GPU-wide before the flag

@@ -133,6 +133,31 @@ __device__ __forceinline__ lane_geom<1> group_geom(const strip_task& t, int grou
     return g;
 }
 
+// Banded geometry for a narrow strip (nx <= 14 own words, one word per lane):
+// the warp holds `bands` side-by-side copies of the strip's segment, each
+// nx + 2 lanes wide with a halo word at either end, and copy q sweeps output
+// rows t.y0 + q*t.ny .. + t.ny of the same columns (clipped to the grid), so
+// a narrow strip fills the warp instead of idling most of its lanes.  Lanes
+// past the last copy compute a duplicate of copy 0's words and store nothing.
+__device__ __forceinline__ lane_geom<1> band_geom(const strip_task& t, int bands, int lane) {
+    lane_geom<1> g;
+    const int s = t.nx + 2;
+    int q = lane / s;
+    const int i = lane - q * s;
+    const bool live = q < bands;
+    if (!live) q = 0;
+    int c = (t.x0 - 1 + i) % t.wd;
+    if (c < 0) c += t.wd;
+    g.col[0] = c;
+    g.src_l = q * s + (i > 0 ? i - 1 : 0);
+    g.src_r = q * s + (i < s - 1 ? i + 1 : i);
+    g.yoff = q * t.ny;
+    const int rows_left = t.h - (t.y0 + g.yoff);
+    g.rows = live ? (rows_left < t.ny ? (rows_left > 0 ? rows_left : 0) : t.ny) : 0;
+    g.keep[0] = live && i >= 1 && i <= t.nx;
+    return g;
+}
+
 // Per-level lane keys of a window rule that draws random numbers
 // (R::level_keys); nothing for the other rules.
 struct no_keys {

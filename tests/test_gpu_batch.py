@@ -56,6 +56,25 @@ def test_narrow_grids_use_exact_wrap_groups(cuda):
         assert (g.cells() == O.run_standard(a, c, s)).all(), (a, x, y, s)
 
 
+@pytest.mark.parametrize("opts", [dict(), dict(temporal_steps=4, tile_rows=24), dict(temporal_steps=8, tile_rows=13),
+                                  dict(temporal_steps=32, tile_rows=40)])
+def test_narrow_last_strips_run_as_row_bands(cuda, opts):
+    # widths of 31..75 words: last strips of 1..14 own words run as 2..10 row
+    # bands side by side in the warp, wider ones as one strip; heights from a
+    # few rows (fewer rows than bands) to several tile rows, with band counts
+    # that divide the tile height or not
+    specs = [(w % 3, 32 * w, h) for w in range(31, 76) for h in (1 + (w * 7) % 23, 150)]
+    steps = [1 + (i * 13) % 40 for i in range(len(specs))]
+    grids, cells = make_grids(specs, 300)
+    with cb.Batch(grids, steps, **opts) as b:
+        b.run()
+        b.wait()
+    for (a, x, y), g, c, s in zip(specs, grids, cells, steps):
+        assert (g.cells() == O.run_standard(a, c, s)).all(), (a, x, y, s, opts)
+    for g in grids:
+        g.close()
+
+
 def test_replays_continue_and_match_per_grid_path(cuda):
     rng = random.Random(5)
     specs = random_specs(rng, 24, max_words=70, max_rows=70)
