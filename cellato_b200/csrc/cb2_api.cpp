@@ -114,8 +114,10 @@ static bool tuned_entry(int automaton, int64_t x, int64_t y, cb2_tuning* out) {
 static bool valid_k(int k) { return k == 1 || k == 2 || k == 4 || k == 8 || k == 16 || k == 32; }
 
 // Default (K, V, L, rows per step) per automaton, the fastest plans measured
-// on B200 at the headline sizes; cb2_autotune replaces them per size.
-static const int kDefaultPlan[kNumBuiltin][4] = {{32, 2, 16, 4}, {32, 1, 16, 4}, {32, 2, 16, 4}};
+// on B200 at the headline sizes; cb2_autotune replaces them per size.  (The
+// shift-register Greenberg-Hastings network needs a fourth register per level
+// and word, so its 16-level shape spills; 8 levels per warp is fastest.)
+static const int kDefaultPlan[kNumBuiltin][4] = {{32, 2, 16, 4}, {32, 1, 16, 4}, {32, 2, 8, 4}};
 // Lowered DSL automata: a window of 3P words per row and level keeps the
 // register count in check only for short chains.
 static const int kDefaultDslPlan[4] = {8, 1, 2, 2};
@@ -698,9 +700,10 @@ int cb2_measure_lop3_peak(double* ops_per_second) {
 int cb2_network_ops(int automaton, double* alu, double* shuffles) {
     // Per 32-bit word per generation (cb2_rules.cuh): two funnel shifts for
     // the west/east neighbour words, plus the rule's logic ops (game of life
-    // 10, wireworld 10, greenberg-hastings 7 three-input operations); two
-    // shuffles per lane per row, shared by the lane's V = 2 words.
-    static const double kLogic[kNumBuiltin] = {10, 10, 7};
+    // 10, wireworld 10, greenberg-hastings 5 three-input operations on its
+    // shift-register encoding); two shuffles per lane per row, shared by the
+    // lane's V = 2 words.
+    static const double kLogic[kNumBuiltin] = {10, 10, 5};
     if (automaton >= kNumBuiltin && automaton < automaton_count())
         return fail(CB2_EINVAL, "no static operation count for a lowered DSL automaton");
     if (automaton < 0 || automaton >= kNumBuiltin) return fail(CB2_ENOTFOUND, "unknown automaton");

@@ -85,6 +85,15 @@ __device__ __forceinline__ void slot_write(uint32_t* slot, int lane, const uint3
     }
 }
 
+// A row read from the input ring enters the first level in the rule's
+// working encoding (encode_states; the identity for most rules).
+template <class R, int V>
+__device__ __forceinline__ void input_row(const uint32_t* slot, int lane, uint32_t (&row)[V][R::P]) {
+    slot_read<R, V>(slot, lane, row);
+#pragma unroll
+    for (int i = 0; i < V; ++i) encode_states<R>(row[i]);
+}
+
 // Runs one strip task on the whole CTA (W = K / L warps, all active).
 // `smem` holds pipe_smem_words<R, K, V, L, DEPTH>() words, 16-byte aligned.
 template <class R, int K, int V, int L, int DEPTH>
@@ -150,7 +159,7 @@ __device__ __forceinline__ void pipe_run(const strip_task& t, uint32_t* smem) {
         if (warp == 0) {
             issue(st + DEPTH - 1);
             cp_async_wait<DEPTH - 1>();
-            if (st < total) slot_read<R, V>(ring + (st % DEPTH) * SLOT, lane, row);
+            if (st < total) input_row<R, V>(ring + (st % DEPTH) * SLOT, lane, row);
             else
 #pragma unroll
                 for (int i = 0; i < V; ++i)
@@ -306,7 +315,7 @@ __device__ __forceinline__ void pipe_run_rows(const strip_task& t, const lane_ge
                 for (int j = 0; j < RPS; ++j) {
                     const int r = RPS * st + j;
                     if (r < total) {
-                        slot_read<R, V>(ring + (r % DEPTH) * SLOT, lane, rows[j]);
+                        input_row<R, V>(ring + (r % DEPTH) * SLOT, lane, rows[j]);
                     } else {
 #pragma unroll
                         for (int i = 0; i < V; ++i)
@@ -436,7 +445,7 @@ __device__ __forceinline__ void warp_run(const strip_task& t, const lane_geom<V>
         constexpr int S = decltype(parity)::value;
         issue(st + DEPTH - 1);
         cp_async_wait<DEPTH - 1>();
-        if (st < total) slot_read<R, V>(smem + (st % DEPTH) * SLOT, lane, pend[0]);
+        if (st < total) input_row<R, V>(smem + (st % DEPTH) * SLOT, lane, pend[0]);
         uint32_t out[V][P];
         skewed_step<R, K, V, S>(s, pend, out, geom.src_l, geom.src_r);
         const int j = st - 2 * K + 1;  // output sweep row

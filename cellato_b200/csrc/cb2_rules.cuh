@@ -25,6 +25,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 
 #if defined(__CUDACC__)
 #define CB2_HD __host__ __device__ __forceinline__
@@ -144,22 +145,67 @@ struct wire {
 };
 
 // Greenberg-Hastings excitable medium, P = 3 (quiescent=0, excited=1,
-// refractory 2..7).
+// refractory 2..7).  Inside a launch a cell's three bits are a de Bruijn
+// shift register instead of its dictionary index: the cycle q -> e -> r1 ->
+// ... -> r6 -> q is the sequence of 3-bit windows of the cyclic word
+// 00010111 (as s2 s1 s0: q=000 e=001 r1=010 r2=101 r3=011 r4=111 r5=110
+// r6=100), so a generation moves s1 to s2 and s0 to s1 and computes one new
+// s0.  Per word and generation that is 5 LOP3 + 2 funnel shifts against
+// 7 + 2 on the dictionary indexes; the three planes are re-encoded as rows
+// enter a launch and decoded as they are stored (3 LOP3 each way, once per
+// launch of K generations).
 struct excitable {
     static constexpr int P = 3;
     static constexpr int NH = 1;
     static constexpr int id = 2;
     static constexpr bool kWindow = false;
-    CB2_HD static uint32_t indicator(const uint32_t (&s)[P]) { return s[0] & ~s[1] & ~s[2]; }  // excited
-    CB2_HD static void hagg(uint32_t l, uint32_t c, uint32_t r, uint32_t (&h)[NH]) { h[0] = l | c | r; }
-    // 0 -> 1 iff any excited neighbour; s -> s+1 for 1..6; 7 -> 0.
+    static constexpr bool kCodec = true;
+    // dictionary index bits (r2 r1 r0) -> shift register (s2 s1 s0)
+    CB2_HD static void encode(uint32_t (&s)[P]) {
+        const uint32_t r0 = s[0], r1 = s[1], r2 = s[2];
+        s[0] = lop3<0x3A>(r2, r1, r0);
+        s[1] = lop3<0x74>(r2, r1, r0);
+        s[2] = lop3<0xE8>(r2, r1, r0);
+    }
+    // shift register (s2 s1 s0) -> dictionary index bits (r2 r1 r0)
+    CB2_HD static void decode(uint32_t (&s)[P]) {
+        const uint32_t s0 = s[0], s1 = s[1], s2 = s[2];
+        s[0] = lop3<0xB2>(s2, s1, s0);
+        s[1] = lop3<0x74>(s2, s1, s0);
+        s[2] = lop3<0xD8>(s2, s1, s0);
+    }
+    // excited: s2 s1 s0 = 001
+    CB2_HD static uint32_t indicator(const uint32_t (&s)[P]) { return lop3<0x10>(s[0], s[1], s[2]); }
+    CB2_HD static void hagg(uint32_t l, uint32_t c, uint32_t r, uint32_t (&h)[NH]) { h[0] = lop3<0xFE>(l, c, r); }
+    // 0 -> 1 iff any excited neighbour; s -> s+1 for 1..6; 7 -> 0.  The new s0
+    // is "any" for q (000) and the sequence's next bit otherwise (1 after 010,
+    // 011 and 101): s2 ? s0 & G : s0 ^ G with G = s0 ? ~s1 : s1 | any.
     CB2_HD static void next(const uint32_t (&a)[NH], const uint32_t (&m)[NH], const uint32_t (&b)[NH],
                             const uint32_t (&c)[P], uint32_t (&o)[P]) {
-        uint32_t any = a[0] | m[0] | b[0];
-        o[0] = ~c[0] & (c[1] | c[2] | any);
-        o[1] = c[1] ^ c[0];
-        o[2] = c[2] ^ (c[1] & c[0]);
+        const uint32_t any = lop3<0xFE>(a[0], m[0], b[0]);
+        const uint32_t g = lop3<0x3E>(c[1], c[0], any);
+        o[0] = lop3<0x86>(c[2], c[0], g);
+        o[1] = c[0];
+        o[2] = c[1];
     }
 };
+
+// Rules that keep their states in another encoding inside a launch
+// (R::kCodec: R::encode as rows enter the first level, R::decode as finished
+// rows are stored), so that grids in memory always hold dictionary indexes;
+// the other rules work on the indexes themselves.
+template <class R, class = void>
+struct has_codec : std::false_type {};
+template <class R>
+struct has_codec<R, std::void_t<decltype(R::kCodec)>> : std::bool_constant<R::kCodec> {};
+
+template <class R>
+CB2_HD void encode_states(uint32_t (&s)[R::P]) {
+    if constexpr (has_codec<R>::value) R::encode(s);
+}
+template <class R>
+CB2_HD void decode_states(uint32_t (&s)[R::P]) {
+    if constexpr (has_codec<R>::value) R::decode(s);
+}
 
 } // namespace cb2

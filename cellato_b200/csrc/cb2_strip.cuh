@@ -301,17 +301,25 @@ __device__ __forceinline__ void skewed_step(strip_state<R, K, V>& s, uint32_t (&
             for (int p = 0; p < R::P; ++p) pend[g][i][p] = pend[g - 1][i][p];
 }
 
-// Stores the lane's words of output row t.y0 + geom.yoff + j (0 <= j < geom.rows).
+// Stores the lane's words of output row t.y0 + geom.yoff + j (0 <= j < geom.rows),
+// back in dictionary indexes (decode_states).
 template <class R, int V>
 __device__ __forceinline__ void strip_store(const strip_task& t, const lane_geom<V>& geom, int j,
                                             const uint32_t (&src)[V][R::P]) {
     if (j >= geom.rows) return;
     uint32_t* base = t.out + (int64_t)(t.y0 + geom.yoff + j) * t.wd;
+    uint32_t w[V][R::P];
+#pragma unroll
+    for (int i = 0; i < V; ++i) {
+#pragma unroll
+        for (int p = 0; p < R::P; ++p) w[i][p] = src[i][p];
+        decode_states<R>(w[i]);
+    }
 #pragma unroll
     for (int p = 0; p < R::P; ++p)
 #pragma unroll
         for (int i = 0; i < V; ++i)
-            if (geom.keep[i]) base[p * t.plane_words + geom.col[i]] = src[i][p];
+            if (geom.keep[i]) base[p * t.plane_words + geom.col[i]] = w[i][p];
 }
 
 } // namespace cb2

@@ -40,10 +40,25 @@ static int run(int x, int y, int steps) {
     int xw = x / 32;
     std::vector<uint32_t> a((size_t)R::P * xw * y), b(a.size());
     if (fread(a.data(), 4, a.size(), stdin) != a.size()) return 2;
+    // the kernels' working encoding of the states (cb2::encode_states), as a launch enters and leaves it
+    auto recode = [&](bool enc) {
+        const size_t plane = (size_t)xw * y;
+        for (size_t w = 0; w < plane; ++w) {
+            uint32_t s[R::P];
+            for (int p = 0; p < R::P; ++p) s[p] = a[p * plane + w];
+            if (enc)
+                cb2::encode_states<R>(s);
+            else
+                cb2::decode_states<R>(s);
+            for (int p = 0; p < R::P; ++p) a[p * plane + w] = s[p];
+        }
+    };
+    recode(true);
     for (int s = 0; s < steps; ++s) {
         step<R>(a, b, xw, y);
         a.swap(b);
     }
+    recode(false);
     fwrite(a.data(), 4, a.size(), stdout);
     return 0;
 }
