@@ -23,7 +23,9 @@ roofline  the strip kernel against the measured integer-logic peak (the
 cpu_baseline  Cellato's own CPU traverser (oracle/_ref, compiled from the
           reference headers) on the benchmark grid itself, on the host cores:
           all threads (each on a band of the grid's rows) and one thread (the
-          whole grid), over a timed sub-range of the step's generations.
+          whole grid), over a timed sub-range of the step's generations, in
+          its fastest layout (bit_planes, 64-bit words); and one thread in the
+          standard layout on a 64-row band of the grid.
 workloads  (one GPU) the WireWorld and Greenberg-Hastings 32768^2 x 2000
           workloads, each with its own roofline, e2e and clocks.
 temporal_depths  (one GPU) the headline at k = 1, 2, 4, 8 generations per
@@ -210,14 +212,37 @@ class ReferenceSample:
         return (f"{where}; {what}; {s['gens']} of the step's {self.gens} generations timed ({s['secs']:.2f} s), "
                 f"a full step extrapolated at that rate to {full_s:.1f} s; host CPU {cpu_model()}")
 
+    def standard_sample(self, target_s: float, rows: int = 64) -> dict:
+        """One thread, the reference traverser with the standard layout (a byte
+        per cell, the per-cell evaluator: Cellato's reference configuration) on
+        the first `rows` rows of the grid as a torus of its own."""
+        import numpy as np
+
+        rows = min(rows, self.y)
+        band = np.ascontiguousarray(self.planes[:, :rows, :])
+        cells = self.O.unpack("bit_planes", band, self.x, rows, self.P, 32)
+        probe = max(self.O.ref_bench(self.a, cells, 1, 1, layout="standard"), 1e-4)
+        gens = max(1, min(self.gens, int(target_s / probe)))
+        secs = self.O.ref_bench(self.a, cells, gens, 1, layout="standard")
+        full_s = secs * self.gens / gens * self.y / rows
+        return {"value": self.x * rows * gens / secs / 1e9, "unit": METRIC, "cores": 1,
+                "sample": (f"1 host thread, Cellato CPU simple traverser, standard layout (one byte per cell), on a "
+                           f"{self.x}x{rows} band of the {self.x}x{self.y} grid (a torus of its own); {gens} "
+                           f"generations timed ({secs:.2f} s), a full step of the whole grid extrapolated at that "
+                           f"rate to {full_s:.0f} s; host CPU {cpu_model()}")}
+
     def baseline(self, target_s: float) -> dict:
-        """cpu_baseline of the B200 arm: the all-threads aggregate, and one thread."""
+        """cpu_baseline of the B200 arm: the all-threads aggregate, one thread,
+        and one thread with the reference's standard layout."""
         agg = self.sample(target_s, self.threads)
         one = self.sample(min(target_s, 4.0), 1) if self.threads > 1 else agg
-        return {"value": agg["value"], "unit": METRIC, "cores": agg["threads"], "kind": self.kind,
-                "sample": self.describe(agg),
-                "single_core": {"value": one["value"], "unit": METRIC, "cores": 1, "sample": self.describe(one)},
-                "cpu_model": cpu_model()}
+        out = {"value": agg["value"], "unit": METRIC, "cores": agg["threads"], "kind": self.kind,
+               "sample": self.describe(agg),
+               "single_core": {"value": one["value"], "unit": METRIC, "cores": 1, "sample": self.describe(one)},
+               "cpu_model": cpu_model()}
+        if self.kind == "reference":
+            out["single_core_standard_layout"] = self.standard_sample(min(target_s, 2.0))
+        return out
 
 
 def reference_arm(args, wl) -> None:
