@@ -114,10 +114,10 @@ static bool tuned_entry(int automaton, int64_t x, int64_t y, cb2_tuning* out) {
 static bool valid_k(int k) { return k == 1 || k == 2 || k == 4 || k == 8 || k == 16 || k == 32; }
 
 // Default (K, V, L, rows per step) per automaton, the fastest plans measured
-// on B200 at the headline sizes; cb2_autotune replaces them per size.  (The
-// shift-register Greenberg-Hastings network needs a fourth register per level
-// and word, so its 16-level shape spills; 8 levels per warp is fastest.)
-static const int kDefaultPlan[kNumBuiltin][4] = {{32, 2, 16, 4}, {32, 1, 16, 4}, {32, 2, 8, 4}};
+// on B200 at the headline sizes; cb2_autotune replaces them per size.
+// (Greenberg-Hastings: 16 generations in one warp of 16 levels, one CTA per
+// warp, so no barrier between warps.)
+static const int kDefaultPlan[kNumBuiltin][4] = {{32, 2, 16, 4}, {32, 1, 16, 4}, {16, 2, 16, 4}};
 // Lowered DSL automata: a window of 3P words per row and level keeps the
 // register count in check only for short chains.
 static const int kDefaultDslPlan[4] = {8, 1, 2, 2};

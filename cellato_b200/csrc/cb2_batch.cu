@@ -46,6 +46,8 @@
 // (from the grid's run start and its chunk split) and the grid's seed, which
 // stochastic and time-dependent rules read; the run start advances on the
 // device after each run, so replays continue the grids' time.
+// The batch kernels keep plain copies of the planes a rule passes on (cb2_rules.cuh fresh).
+#define CB2_PLAIN_COPIES
 #include "cellato_b200.h"
 
 #include <cuda_runtime.h>

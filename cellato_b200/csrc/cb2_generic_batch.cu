@@ -9,6 +9,8 @@
 //
 // Built only when the Cellato headers are present; cb2_generic_none.cpp
 // stands in otherwise and reports no kernel.
+// The batch kernels keep plain copies of the planes a rule passes on (cb2_rules.cuh fresh).
+#define CB2_PLAIN_COPIES
 #include <cuda_runtime.h>
 
 #include <type_traits>

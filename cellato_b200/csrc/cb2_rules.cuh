@@ -110,6 +110,28 @@ struct game_of_life {
     }
 };
 
+#if defined(__CUDACC__)
+// A 1 the compiler cannot see through (constant memory, set when the module
+// loads); one per translation unit.
+static __constant__ uint32_t cb2_unit = 1;
+#endif
+// x as a new value: a multiply by cb2_unit, on the FMA pipe that the networks
+// leave idle.  A plane a rule passes on unchanged otherwise stays one value
+// over several levels of the wavefront, and the registers of the unrolled
+// levels cannot follow it (the shift-register Greenberg-Hastings network below
+// needed a fourth register per level and word: 255 and spills at 16 levels
+// per warp and two words per lane, 228 and none with fresh copies).  The batch
+// kernels (one word per lane, eight levels per warp, ~120 registers) are not
+// short of registers, so their translation units define CB2_PLAIN_COPIES and
+// keep plain copies instead of the extra multiplies.
+CB2_HD uint32_t fresh(uint32_t x) {
+#if defined(__CUDA_ARCH__) && !defined(CB2_PLAIN_COPIES)
+    return x * cb2_unit;
+#else
+    return x;
+#endif
+}
+
 // WireWorld, P = 2 (empty=0, head=1, tail=2, conductor=3).  Ten LOP3 and
 // two funnel shifts per word and generation, each written as one lop3.
 struct wire {
@@ -138,7 +160,7 @@ struct wire {
         const uint32_t y = lop3<0xE8>(a[1], m[1], b[1]);
         const uint32_t g = lop3<0x16>(p0, k0, x);      // p0 ? ~k0 & ~x : k0 ^ x
         const uint32_t one_or_two = lop3<0x30>(g, y, g);  // g & ~y
-        o[0] = c[1];
+        o[0] = fresh(c[1]);
         // (c0 ^ c1) | (c0 & c1 & ~one_or_two): head -> tail (2), tail -> conductor (3), conductor -> 1 or 3
         o[1] = lop3<0x7C>(c[0], c[1], one_or_two);
     }
@@ -185,8 +207,8 @@ struct excitable {
         const uint32_t any = lop3<0xFE>(a[0], m[0], b[0]);
         const uint32_t g = lop3<0x3E>(c[1], c[0], any);
         o[0] = lop3<0x86>(c[2], c[0], g);
-        o[1] = c[0];
-        o[2] = c[1];
+        o[1] = fresh(c[0]);
+        o[2] = fresh(c[1]);
     }
 };
 

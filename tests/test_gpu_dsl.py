@@ -166,6 +166,34 @@ def test_batch_kernel_runs_dsl_automata(ref, opts):
         g.close()
 
 
+@pytest.mark.parametrize("name", ["lightning-forest", "critters", "traffic", "noisy-life"])
+def test_batch_banded_last_strips_of_lowered_rules(ref, name):
+    # widths whose last strip (1..14 words) runs as 2..10 row bands side by side
+    # in the warp: stochastic draws (paired or not, by the bands' lane parity),
+    # Margolus blocks and the alternating rule must see the same global cells,
+    # rows and generations as in one strip; tiles of 16 rows give several bands
+    # per tile row, and ragged last tiles
+    rng = random.Random(sum(map(ord, name)))
+    cases = []
+    for i, w in enumerate((31, 33, 38, 44, 46, 61)):
+        y = (50, 33, 70, 17, 64, 29)[i]
+        cases.append((32 * w, y, rng.randrange(1, 30), rng.randrange(1, 1 << 31), cells_for(name, 32 * w, y, 400 + i)))
+    grids = []
+    for x, y, steps, seed, cells in cases:
+        g = cb.DeviceGrid(name, x, y)
+        g.upload_cells(cells)
+        g.set_seed(seed)
+        grids.append(g)
+    with cb.Batch(grids, [c[2] for c in cases], temporal_steps=8, tile_rows=16) as b:
+        b.run()
+        b.wait()
+    for g, (x, y, steps, seed, cells) in zip(grids, cases):
+        want, want_ck = ref.ref_run_named(name, cells, steps, seed=seed)
+        assert (g.cells() == want).all(), (name, x, y, steps)
+        assert g.checksum_str() == want_ck, (name, x, y)
+        g.close()
+
+
 def test_batch_follows_time_and_seed_set_between_runs(ref):
     # a grid re-timed and re-seeded between runs: the next run rebuilds the
     # schedule and must equal the strip kernels from that generation and seed
