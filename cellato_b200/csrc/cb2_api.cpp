@@ -116,8 +116,9 @@ static bool valid_k(int k) { return k == 1 || k == 2 || k == 4 || k == 8 || k ==
 // Default (K, V, L, rows per step) per automaton, the fastest plans measured
 // on B200 at the headline sizes; cb2_autotune replaces them per size.
 // (Greenberg-Hastings: 16 generations in one warp of 16 levels, one CTA per
-// warp, so no barrier between warps.)
-static const int kDefaultPlan[kNumBuiltin][4] = {{32, 2, 16, 4}, {32, 1, 16, 4}, {16, 2, 16, 4}};
+// warp, so no barrier between warps; WireWorld: two words per lane, which
+// halves the x-halo, over two warps of 8 levels.)
+static const int kDefaultPlan[kNumBuiltin][4] = {{32, 2, 16, 4}, {16, 2, 8, 4}, {16, 2, 16, 4}};
 // Lowered DSL automata: a window of 3P words per row and level keeps the
 // register count in check only for short chains.
 static const int kDefaultDslPlan[4] = {8, 1, 2, 2};
