@@ -340,6 +340,8 @@ __device__ __forceinline__ void pipe_run_rows(const strip_task& t, const lane_ge
                     rc.y = yglob;
                     next_row();
                     strip_push<R, L, V, 1>(s, rows[j + 1], geom.src_l, geom.src_r, &geom, &rc);
+                } else if constexpr (has_pairs<R>::value) {
+                    strip_push2<R, L, V>(s, rows[j], rows[j + 1], geom.src_l, geom.src_r);
                 } else {
                     strip_push<R, L, V, 0>(s, rows[j], geom.src_l, geom.src_r);
                     strip_push<R, L, V, 1>(s, rows[j + 1], geom.src_l, geom.src_r);

@@ -108,7 +108,38 @@ struct game_of_life {
         uint32_t e = ~(t0 ^ t1) & (t0 ^ t2);  // (t0,t1,t2) is (1,1,0) or (0,0,1)
         o[0] = e & (t0 | c[0]);
     }
+    // Rows in pairs: output rows r and r+1 share census rows r and r+1, so
+    // their 2-bit counts are summed once (Q = 0..6, 4 LOP3) and each output
+    // adds its third row's count z and tests the total in 5 LOP3:
+    //   w  = (q1 ^ z1) ? ~q2 : q1 ^ q2     e  = ~(q1 ^ z1 ^ q0)
+    //   g3 = LUT 0x41 (q0, z0, centre)     g4 = LUT 0x59 (q0, z0, e)
+    //   alive = w & ~g3 & ~g4
+    // (found by exhaustive search over LOP3 circuits, none of 4 gates exists;
+    // checked against T == 3 | (T == 4 & centre) for every count and centre).
+    // Per word and generation 4/2 + 5 + the row's 2 horizontal LOP3 = 9 LOP3
+    // + 2 funnel shifts, against 10 + 2 row by row.
+    static constexpr bool kPairs = true;
+    CB2_HD static void pair(const uint32_t (&x)[NH], const uint32_t (&y)[NH], uint32_t (&q)[3]) {
+        const uint32_t k = x[0] & y[0];
+        q[0] = x[0] ^ y[0];
+        q[1] = xor3(x[1], y[1], k);
+        q[2] = maj3(x[1], y[1], k);
+    }
+    CB2_HD static void next_pair(const uint32_t (&q)[3], const uint32_t (&z)[NH], const uint32_t (&c)[P],
+                                 uint32_t (&o)[P]) {
+        const uint32_t w = lop3<0x56>(q[1], z[1], q[2]);
+        const uint32_t e = lop3<0x69>(q[1], z[1], q[0]);
+        const uint32_t g3 = lop3<0x41>(q[0], z[0], c[0]);
+        const uint32_t g4 = lop3<0x59>(q[0], z[0], e);
+        o[0] = lop3<0x10>(w, g3, g4);
+    }
 };
+
+// Rules that also evaluate rows in pairs (R::kPairs: R::pair, R::next_pair).
+template <class R, class = void>
+struct has_pairs : std::false_type {};
+template <class R>
+struct has_pairs<R, std::void_t<decltype(R::kPairs)>> : std::bool_constant<R::kPairs> {};
 
 #if defined(__CUDACC__)
 // A 1 the compiler cannot see through (constant memory, set when the module

@@ -278,6 +278,63 @@ __device__ __forceinline__ void strip_push(strip_state<R, K, V>& s, uint32_t (&r
     for (int g = 0; g < K; ++g) level_push<R, K, V, Q>(s, g, row, src_l, src_r, geom, rc);
 }
 
+// Two rows through one level, for rules that evaluate rows in pairs
+// (has_pairs): `ra` has parity slot 0 and `rb` slot 1, so before the call slot
+// 0 holds the aggregates of the row above ra's upper neighbour, slot 1 those
+// of ra's upper neighbour (whose states are the centre c[1]).  The census rows
+// shared by the two outputs -- ra's upper neighbour and ra -- are summed once
+// (R::pair); each output adds its third row.  On return ra and rb hold the two
+// rows above them advanced one generation, and the slots the same state as
+// two level_push calls leave (c[0] is not kept: no pair push reads it).
+template <class R, int K, int V>
+__device__ __forceinline__ void level_push2(strip_state<R, K, V>& s, int g, uint32_t (&ra)[V][R::P],
+                                            uint32_t (&rb)[V][R::P], int src_l, int src_r) {
+    constexpr int P = R::P, NH = R::NH;
+    uint32_t ia[V], ib[V];
+#pragma unroll
+    for (int i = 0; i < V; ++i) {
+        ia[i] = R::indicator(ra[i]);
+        ib[i] = R::indicator(rb[i]);
+    }
+    const uint32_t la = __shfl_sync(kFullMask, ia[V - 1], src_l);
+    const uint32_t ra_ = __shfl_sync(kFullMask, ia[0], src_r);
+    const uint32_t lb = __shfl_sync(kFullMask, ib[V - 1], src_l);
+    const uint32_t rb_ = __shfl_sync(kFullMask, ib[0], src_r);
+    uint32_t ha[V][NH], hb[V][NH];
+#pragma unroll
+    for (int i = 0; i < V; ++i) {
+        R::hagg(west_of(i == 0 ? la : ia[i - 1], ia[i]), ia[i], east_of(ia[i], i == V - 1 ? ra_ : ia[i + 1]), ha[i]);
+        R::hagg(west_of(i == 0 ? lb : ib[i - 1], ib[i]), ib[i], east_of(ib[i], i == V - 1 ? rb_ : ib[i + 1]), hb[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < V; ++i) {
+        uint32_t q[3], oa[P], ob[P];
+        R::pair(s.h[g][1][i], ha[i], q);
+        R::next_pair(q, s.h[g][0][i], s.c[g][1][i], oa);
+        R::next_pair(q, hb[i], ra[i], ob);
+#pragma unroll
+        for (int k = 0; k < NH; ++k) {
+            s.h[g][0][i][k] = ha[i][k];
+            s.h[g][1][i][k] = hb[i][k];
+        }
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            s.c[g][1][i][p] = rb[i][p];
+            ra[i][p] = oa[p];
+            rb[i][p] = ob[p];
+        }
+    }
+}
+
+// Two consecutive rows (parity slots 0 and 1) through the K levels, level by
+// level: the same result as strip_push<.., 0>(ra) then strip_push<.., 1>(rb).
+template <class R, int K, int V>
+__device__ __forceinline__ void strip_push2(strip_state<R, K, V>& s, uint32_t (&ra)[V][R::P], uint32_t (&rb)[V][R::P],
+                                            int src_l, int src_r) {
+#pragma unroll
+    for (int g = 0; g < K; ++g) level_push2<R, K, V>(s, g, ra, rb, src_l, src_r);
+}
+
 // Skewed wavefront step: level g takes the row level g-1 produced in the
 // previous step (held in pend[g]), so the K levels of one step are
 // independent of each other.  pend[0] is the new input row; on return

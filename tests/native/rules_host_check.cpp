@@ -30,7 +30,20 @@ static void step(const std::vector<uint32_t>& in, std::vector<uint32_t>& out, in
             agg(r, c, m);
             agg(r + 1, c, b);
             for (int p = 0; p < R::P; ++p) s[p] = in[p * plane + (size_t)r * xw + c];
-            R::next(a, m, b, s, o);
+            if constexpr (cb2::has_pairs<R>::value) {
+                // the kernels' pair path: even rows pair with the row below and add
+                // the row above, odd rows pair with the row above and add the row below
+                uint32_t q[3];
+                if (r % 2 == 0) {
+                    R::pair(m, b, q);
+                    R::next_pair(q, a, s, o);
+                } else {
+                    R::pair(a, m, q);
+                    R::next_pair(q, b, s, o);
+                }
+            } else {
+                R::next(a, m, b, s, o);
+            }
             for (int p = 0; p < R::P; ++p) out[p * plane + (size_t)r * xw + c] = o[p];
         }
 }
