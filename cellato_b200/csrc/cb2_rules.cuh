@@ -96,8 +96,8 @@ struct game_of_life {
     static constexpr bool kWindow = false;  // census network (a window rule sees all planes)
     CB2_HD static uint32_t indicator(const uint32_t (&s)[P]) { return s[0]; }
     CB2_HD static void hagg(uint32_t l, uint32_t c, uint32_t r, uint32_t (&h)[NH]) {
-        h[0] = xor3(l, c, r);
-        h[1] = maj3(l, c, r);
+        h[0] = lop3<0x96>(l, c, r);  // xor3
+        h[1] = lop3<0xE8>(l, c, r);  // majority
     }
     // T == 3 -> alive; T == 4 -> keep centre; otherwise dead.  T <= 9, and the
     // dropped bit 3 cannot alias 3 (11) or 4 (12).
@@ -119,11 +119,13 @@ struct game_of_life {
     // Per word and generation 4/2 + 5 + the row's 2 horizontal LOP3 = 9 LOP3
     // + 2 funnel shifts, against 10 + 2 row by row.
     static constexpr bool kPairs = true;
+    // (written as explicit lop3: with C operators the compiler re-covers the
+    // shared terms and issued 10.4 LOP3 per word-generation, as row by row)
     CB2_HD static void pair(const uint32_t (&x)[NH], const uint32_t (&y)[NH], uint32_t (&q)[3]) {
-        const uint32_t k = x[0] & y[0];
-        q[0] = x[0] ^ y[0];
-        q[1] = xor3(x[1], y[1], k);
-        q[2] = maj3(x[1], y[1], k);
+        const uint32_t k = lop3<0xC0>(x[0], y[0], x[0]);  // x0 & y0
+        q[0] = lop3<0x3C>(x[0], y[0], x[0]);              // x0 ^ y0
+        q[1] = lop3<0x96>(x[1], y[1], k);
+        q[2] = lop3<0xE8>(x[1], y[1], k);
     }
     CB2_HD static void next_pair(const uint32_t (&q)[3], const uint32_t (&z)[NH], const uint32_t (&c)[P],
                                  uint32_t (&o)[P]) {
