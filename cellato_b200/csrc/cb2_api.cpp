@@ -115,10 +115,10 @@ static bool valid_k(int k) { return k == 1 || k == 2 || k == 4 || k == 8 || k ==
 
 // Default (K, V, L, rows per step) per automaton, the fastest plans measured
 // on B200 at the headline sizes; cb2_autotune replaces them per size.
-// (Greenberg-Hastings: 16 generations in one warp of 16 levels, one CTA per
-// warp, so no barrier between warps; WireWorld: two words per lane, which
-// halves the x-halo, over two warps of 8 levels.)
-static const int kDefaultPlan[kNumBuiltin][4] = {{32, 2, 16, 4}, {16, 2, 8, 4}, {16, 2, 16, 4}};
+// (Greenberg-Hastings: 16 generations in one warp of 16 levels, and
+// WireWorld: 32 generations in one warp of 32 levels -- one CTA per warp, so
+// no barrier between warps.)
+static const int kDefaultPlan[kNumBuiltin][4] = {{32, 2, 16, 4}, {32, 1, 32, 4}, {16, 2, 16, 4}};
 // Lowered DSL automata: a window of 3P words per row and level keeps the
 // register count in check only for short chains.
 static const int kDefaultDslPlan[4] = {8, 1, 2, 2};
@@ -700,12 +700,13 @@ int cb2_measure_lop3_peak(double* ops_per_second) {
 
 int cb2_network_ops(int automaton, double* alu, double* shuffles) {
     // Per 32-bit word per generation (cb2_rules.cuh): two funnel shifts for
-    // the west/east neighbour words, plus the rule's logic ops (game of life
-    // 9 with rows evaluated in pairs -- every plan of two or more rows per
-    // step; 10 row by row --, wireworld 10, greenberg-hastings 5 three-input
-    // operations on its shift-register encoding); two shuffles per lane per
-    // row, shared by the lane's V = 2 words.
-    static const double kLogic[kNumBuiltin] = {9, 10, 5};
+    // the west/east neighbour words, plus the rule's logic ops with rows
+    // evaluated in pairs -- every plan of two or more rows per step -- (game
+    // of life 9, 10 row by row; wireworld 8, 10 row by row;
+    // greenberg-hastings 5 three-input operations on its shift-register
+    // encoding); two shuffles per lane per row, shared by the lane's V = 2
+    // words.
+    static const double kLogic[kNumBuiltin] = {9, 8, 5};
     if (automaton >= kNumBuiltin && automaton < automaton_count())
         return fail(CB2_EINVAL, "no static operation count for a lowered DSL automaton");
     if (automaton < 0 || automaton >= kNumBuiltin) return fail(CB2_ENOTFOUND, "unknown automaton");

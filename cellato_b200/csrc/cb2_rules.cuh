@@ -197,6 +197,27 @@ struct wire {
         // (c0 ^ c1) | (c0 & c1 & ~one_or_two): head -> tail (2), tail -> conductor (3), conductor -> 1 or 3
         o[1] = lop3<0x7C>(c[0], c[1], one_or_two);
     }
+    // Rows in pairs (see game_of_life): the two shared rows' head counts x, y
+    // become the planes of their sum Q that the test reads -- Q bit 0, [Q <= 1]
+    // and Q bit 2 (Q bit 1 is not needed), 4 LOP3 -- and each output adds its
+    // third row's count z: the count is 1 or 2 iff LUT 0x86 of (z1, [Q <= 1],
+    // ~q0 & ~q2 & ~z0) (3-gate circuit found by exhaustive search, none of 2
+    // exists; checked for every Q and z).  Per word and generation 1 + 2 +
+    // 4/2 + 3 = 8 LOP3 + 2 funnel shifts, against 10 + 2 row by row.
+    static constexpr bool kPairs = true;
+    CB2_HD static void pair(const uint32_t (&x)[NH], const uint32_t (&y)[NH], uint32_t (&q)[3]) {
+        const uint32_t k = lop3<0xC0>(x[0], y[0], x[0]);  // x0 & y0
+        q[0] = lop3<0x3C>(x[0], y[0], x[0]);              // x0 ^ y0
+        q[1] = lop3<0x01>(x[1], y[1], k);                 // Q <= 1
+        q[2] = lop3<0xE8>(x[1], y[1], k);                 // Q bit 2
+    }
+    CB2_HD static void next_pair(const uint32_t (&q)[3], const uint32_t (&z)[NH], const uint32_t (&c)[P],
+                                 uint32_t (&o)[P]) {
+        const uint32_t g = lop3<0x01>(q[0], q[2], z[0]);
+        const uint32_t one_or_two = lop3<0x86>(z[1], q[1], g);
+        o[0] = fresh(c[1]);
+        o[1] = lop3<0x7C>(c[0], c[1], one_or_two);
+    }
 };
 
 // Greenberg-Hastings excitable medium, P = 3 (quiescent=0, excited=1,

@@ -410,8 +410,9 @@ int cb2_measure_lop3_peak(double* ops_per_second);
 
 /* Logic, shift and shuffle instructions the strip kernel issues per 32-bit
  * word per generation for this automaton (the integer cost of the network),
- * for plans of two or more rows per step; with one row per step game-of-life
- * issues one logic op more (its rows are not evaluated in pairs). */
+ * for plans of two or more rows per step; with one row per step, whose rows
+ * are not evaluated in pairs, game-of-life issues one logic op more and wire
+ * two. */
 int cb2_network_ops(int automaton, double* alu_ops_per_word, double* shuffles_per_word);
 
 #ifdef __cplusplus
