@@ -43,6 +43,11 @@ static const std::vector<strip_variant>& variants_for() {
         make_variant<R, 16, 2, 16, 4>(), make_variant<R, 16, 1, 16, 4>(),
         make_variant<R, 32, 2, 16, 4>(), make_variant<R, 32, 2, 8, 4>(), make_variant<R, 32, 2, 8, 2>(),
         make_variant<R, 32, 2, 4, 4>(), make_variant<R, 32, 1, 16, 4>(), make_variant<R, 32, 1, 32, 4>(),
+        // short chains with two or four rows per step, so that rules which
+        // evaluate rows in pairs (has_pairs) do so at every depth
+        make_variant<R, 1, 2, 1, 2>(), make_variant<R, 1, 2, 1, 4>(), make_variant<R, 2, 2, 2, 2>(),
+        make_variant<R, 2, 2, 2, 4>(), make_variant<R, 2, 2, 1, 4>(), make_variant<R, 4, 2, 4, 4>(),
+        make_variant<R, 4, 2, 2, 4>(), make_variant<R, 8, 2, 8, 4>(), make_variant<R, 8, 2, 4, 4>(),
     };
     return v;
 }
