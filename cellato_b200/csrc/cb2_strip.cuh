@@ -296,15 +296,18 @@ __device__ __forceinline__ void level_push2(strip_state<R, K, V>& s, int g, uint
         ia[i] = R::indicator(ra[i]);
         ib[i] = R::indicator(rb[i]);
     }
-    const uint32_t la = __shfl_sync(kFullMask, ia[V - 1], src_l);
-    const uint32_t ra_ = __shfl_sync(kFullMask, ia[0], src_r);
-    const uint32_t lb = __shfl_sync(kFullMask, ib[V - 1], src_l);
-    const uint32_t rb_ = __shfl_sync(kFullMask, ib[0], src_r);
+    // the neighbour lanes' indicator words next to this lane's, for each row
+    const uint32_t a_west = __shfl_sync(kFullMask, ia[V - 1], src_l);
+    const uint32_t a_east = __shfl_sync(kFullMask, ia[0], src_r);
+    const uint32_t b_west = __shfl_sync(kFullMask, ib[V - 1], src_l);
+    const uint32_t b_east = __shfl_sync(kFullMask, ib[0], src_r);
     uint32_t ha[V][NH], hb[V][NH];
 #pragma unroll
     for (int i = 0; i < V; ++i) {
-        R::hagg(west_of(i == 0 ? la : ia[i - 1], ia[i]), ia[i], east_of(ia[i], i == V - 1 ? ra_ : ia[i + 1]), ha[i]);
-        R::hagg(west_of(i == 0 ? lb : ib[i - 1], ib[i]), ib[i], east_of(ib[i], i == V - 1 ? rb_ : ib[i + 1]), hb[i]);
+        R::hagg(west_of(i == 0 ? a_west : ia[i - 1], ia[i]), ia[i], east_of(ia[i], i == V - 1 ? a_east : ia[i + 1]),
+                ha[i]);
+        R::hagg(west_of(i == 0 ? b_west : ib[i - 1], ib[i]), ib[i], east_of(ib[i], i == V - 1 ? b_east : ib[i + 1]),
+                hb[i]);
     }
 #pragma unroll
     for (int i = 0; i < V; ++i) {
