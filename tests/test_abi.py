@@ -73,8 +73,12 @@ def test_tuning_file_round_trip(tmp_path):
 
 
 def test_network_op_counts():
-    alu, shf = cb.network_ops("game-of-life")
-    assert alu == 12 and shf == 1
+    # logic + funnel-shift ops per word and generation with rows evaluated in
+    # pairs (game of life 9 + 2, wire 8 + 2), and greenberg-hastings' shift
+    # register (5 + 2); one shuffle per word at two words per lane
+    for name, ops in (("game-of-life", 11), ("wire", 10), ("excitable", 7)):
+        alu, shf = cb.network_ops(name)
+        assert alu == ops and shf == 1, name
 
 
 def test_server_rejects_unsupported_chunk_lengths():
