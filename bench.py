@@ -777,7 +777,8 @@ def main() -> None:
     lop3_peak = cb.measure_lop3_peak()
     head = measure(cb, torch, ranks, wl, args, rank, world, local_rank, stream, lop3_peak)
 
-    # BASELINE's other single-grid configs, and the headline at each fixed temporal depth
+    # the other single-grid workloads (WireWorld and Greenberg-Hastings 32768^2), and the headline
+    # at each fixed temporal depth
     workloads, depths = None, None
     if world == 1 and not args.no_extra_workloads and args.workload == "gol-65536":
         workloads = {}
