@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 #include <vector>
 
 #include "../../cellato_b200/csrc/cb2_rules.cuh"
@@ -76,7 +77,51 @@ static int run(int x, int y, int steps) {
     return 0;
 }
 
+// Exhaustive check of a rule's pair evaluation (cb2::has_pairs): every
+// combination of the three census rows' 3-cell patterns and the centre state,
+// one combination per bit of the words, against next() on the same rows, for
+// both ways the kernels pair rows (the shared rows with the one above or below).
+template <class R>
+static int check_pairs(const char* name) {
+    if constexpr (cb2::has_pairs<R>::value) {
+        // 3 rows x 3 cells of indicator bits and P centre planes: 9 + P bits per case
+        constexpr int kBits = 9 + R::P;
+        long bad = 0, cases = 0;
+        for (long base = 0; base < (1L << kBits); base += 32) {
+            uint32_t cell[9] = {}, cen[R::P] = {};
+            for (int b = 0; b < 32 && base + b < (1L << kBits); ++b) {
+                const long v = base + b;
+                for (int k = 0; k < 9; ++k) cell[k] |= (uint32_t)((v >> k) & 1) << b;
+                for (int p = 0; p < R::P; ++p) cen[p] |= (uint32_t)((v >> (9 + p)) & 1) << b;
+            }
+            // row r's aggregate of its three indicator cells (the kernels' hagg)
+            uint32_t h[3][R::NH];
+            for (int r = 0; r < 3; ++r) R::hagg(cell[3 * r], cell[3 * r + 1], cell[3 * r + 2], h[r]);
+            uint32_t want[R::P], got_lo[R::P], got_hi[R::P], q[3];
+            R::next(h[0], h[1], h[2], cen, want);
+            R::pair(h[1], h[2], q);  // the output pairs its own row with the row below
+            R::next_pair(q, h[0], cen, got_lo);
+            R::pair(h[0], h[1], q);  // ... or with the row above
+            R::next_pair(q, h[2], cen, got_hi);
+            const uint32_t live = base + 32 <= (1L << kBits) ? 0xffffffffu : (1u << ((1L << kBits) - base)) - 1;
+            for (int p = 0; p < R::P; ++p) {
+                uint32_t diff = ((want[p] ^ got_lo[p]) | (want[p] ^ got_hi[p])) & live;
+                bad += __builtin_popcount(diff);
+            }
+            cases += __builtin_popcount(live);
+        }
+        printf("%s pairs: %ld cases, %ld mismatches\n", name, cases, bad);
+        return bad ? 3 : 0;
+    } else {
+        printf("%s evaluates no pairs\n", name);
+        return 0;
+    }
+}
+
 int main(int argc, char** argv) {
+    if (argc == 2 && std::string(argv[1]) == "pairs")
+        return check_pairs<cb2::game_of_life>("game-of-life") | check_pairs<cb2::wire>("wire") |
+               check_pairs<cb2::excitable>("excitable");
     if (argc != 5) return 1;
     int aut = atoi(argv[1]), x = atoi(argv[2]), y = atoi(argv[3]), steps = atoi(argv[4]);
     switch (aut) {

@@ -35,3 +35,11 @@ def test_networks_match_oracle(checker, automaton):
                              capture_output=True, check=True).stdout
         got = O.unpack("bit_planes", np.frombuffer(out, np.uint8), x, y, P, 32)
         assert (got == O.run_standard(automaton, cells, steps)).all(), (x, y, steps)
+
+
+def test_pair_networks_exhaustive(checker):
+    # the pair evaluation of game-of-life and wire (kernels with two or more rows
+    # per step) equals the row-by-row network on every census pattern and centre
+    out = subprocess.run([checker, "pairs"], capture_output=True, text=True, check=True).stdout
+    assert "game-of-life pairs: 1024 cases, 0 mismatches" in out, out
+    assert "wire pairs: 2048 cases, 0 mismatches" in out, out
